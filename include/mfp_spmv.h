@@ -1,0 +1,360 @@
+/*
+ * mfp_spmv.h — C ABI of the B200 (sm_100a) SpMV engine.
+ *
+ * Drop-in boundary for the per-format SpMV path of
+ * gevtushenko/matrix_format_performance.  The reference exposes that path as
+ * C++ templates (gpu/gpu_matrix_multiplier.h:14-152, gpu/csr_adaptive_spmv.h:13-23,
+ * gpu/scoo_spmv.h:12-23) over the layouts built by common/matrix_converter.cpp
+ * and common/scoo_matrix_class.cpp.  This header flattens that surface into
+ * plain C: pointers, sizes, an int status, and opaque handles.  The C++
+ * compatibility headers under matrix_format_performance_b200/csrc/compat/
+ * rebuild the reference's template signatures on top of it.
+ *
+ * Conventions
+ *  - Every function returns an int status (mfp_status).  On failure a message
+ *    is available from mfp_last_error() (thread-local).
+ *  - "device" pointers are CUDA global-memory addresses on the current device;
+ *    "host" pointers are ordinary process memory.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Device-pointer entry points only enqueue work; they never synchronise.
+ *  - Index arrays are uint32 (the reference uses unsigned int,
+ *    common/matrix_converter.h:36-38).  Value arrays are float (f32) or
+ *    double (f64), as the reference instantiates (gpu_matrix_multiplier.cu:1219-1302).
+ *  - Device arrays passed to the SpMV entry points should start on a 16-byte
+ *    boundary (cudaMalloc gives 256); unaligned arrays take a slower path.
+ */
+#ifndef MFP_SPMV_H
+#define MFP_SPMV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFP_VERSION 100
+
+typedef enum mfp_status {
+  MFP_SUCCESS = 0,
+  MFP_ERROR_INVALID_VALUE = 1,  /* null pointer, inconsistent sizes, bad enum */
+  MFP_ERROR_CUDA = 2,           /* a CUDA runtime call failed */
+  MFP_ERROR_OUT_OF_MEMORY = 3,  /* device or host allocation failed */
+  MFP_ERROR_TOO_LARGE = 4,      /* layout would exceed 32-bit indexing or memory */
+  MFP_ERROR_NOT_SUPPORTED = 5,  /* e.g. a non-general storage scheme */
+  MFP_ERROR_DEVICE_WAIT = 6     /* a bounded device-side wait gave up */
+} mfp_status;
+
+typedef enum mfp_value_type { MFP_F32 = 0, MFP_F64 = 1 } mfp_value_type;
+
+/* ------------------------------------------------------------------------- */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------- */
+int mfp_version(void);
+const char *mfp_status_string(int status);
+const char *mfp_last_error(void);
+
+typedef struct mfp_device_info {
+  int device;
+  int sm_count;                  /* cudaDeviceProp::multiProcessorCount */
+  uint64_t shared_mem_per_block; /* cudaDeviceProp::sharedMemPerBlock (48 KiB) */
+  uint64_t shared_mem_optin;     /* sharedMemPerBlockOptin (227 KiB on B200) */
+  uint64_t l2_bytes;
+  uint64_t global_mem_bytes;
+  int cc_major, cc_minor;
+} mfp_device_info;
+/* Replaces the property query in main.cpp:416-421. */
+int mfp_get_device_info(int device, mfp_device_info *out);
+
+/* ------------------------------------------------------------------------- */
+/* Host-side format construction, bit-exact with the reference converters.   */
+/* All arrays here are HOST arrays sized by the caller.                      */
+/* ------------------------------------------------------------------------- */
+
+/* csr_matrix_class<T>(matrix_class) — common/matrix_converter.cpp:15-87.
+ * Input: COO triplets with double values (matrix_market::matrix_class).
+ * Output: row_ptr[rows+1], columns[nnz], data[nnz]; columns sorted per row.
+ * storage_scheme != 0 (non-general) -> MFP_ERROR_NOT_SUPPORTED, as the
+ * reference throws at matrix_converter.cpp:19-20. */
+int mfp_csr_from_coo_f32(uint32_t rows, uint32_t cols, uint32_t nnz, int storage_scheme,
+                         const uint32_t *row_ids, const uint32_t *col_ids, const double *values,
+                         uint32_t *row_ptr, uint32_t *columns, float *data);
+int mfp_csr_from_coo_f64(uint32_t rows, uint32_t cols, uint32_t nnz, int storage_scheme,
+                         const uint32_t *row_ids, const uint32_t *col_ids, const double *values,
+                         uint32_t *row_ptr, uint32_t *columns, double *data);
+
+/* matrix_rows_statistic / get_rows_statistics — matrix_converter.h:12-22,
+ * matrix_converter.cpp:95-127 (integer average, population std deviation). */
+typedef struct mfp_rows_statistic {
+  uint32_t min_elements_in_rows;
+  uint32_t max_elements_in_rows;
+  uint32_t avg_elements_in_rows;
+  double elements_in_rows_std_deviation;
+} mfp_rows_statistic;
+int mfp_get_rows_statistics(uint32_t rows, const uint32_t *row_ptr, mfp_rows_statistic *out);
+
+/* ell_matrix_class<T> — matrix_converter.cpp:129-203.  Column-major
+ * [k*rows + row], padding col=0 / value=0.  width = max row length for the
+ * plain constructor (mfp_ell_width), or any fixed width (extra elements of a
+ * row are dropped, matrix_converter.cpp:194-199).  Outputs sized width*rows. */
+int mfp_ell_width(uint32_t rows, const uint32_t *row_ptr, uint32_t *width);
+int mfp_ell_from_csr_f32(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const float *data, uint32_t width, float *ell_data, uint32_t *ell_columns);
+int mfp_ell_from_csr_f64(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const double *data, uint32_t width, double *ell_data,
+                         uint32_t *ell_columns);
+
+/* coo_matrix_class<T> — matrix_converter.cpp:211-280.  element_start = 0 gives
+ * every element; element_start = k keeps the elements at in-row position >= k
+ * (the hybrid tail).  Row-major, rows ascending, columns ascending per row. */
+int mfp_coo_count(uint32_t rows, const uint32_t *row_ptr, uint32_t element_start, uint32_t *count);
+int mfp_coo_from_csr_f32(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const float *data, uint32_t element_start, float *coo_data,
+                         uint32_t *coo_cols, uint32_t *coo_rows);
+int mfp_coo_from_csr_f64(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const double *data, uint32_t element_start, double *coo_data,
+                         uint32_t *coo_cols, uint32_t *coo_rows);
+
+/* hybrid_matrix_class<T>::allocate width rule — matrix_converter.cpp:288-310:
+ * width = (unsigned)(avg + (max - avg) * percent), avg the integer average. */
+int mfp_hybrid_width(uint32_t rows, const uint32_t *row_ptr, double percent, uint32_t *width);
+/* Engine extension (no reference counterpart): the q-quantile of the row
+ * lengths (q = 2/3 for the power-law configuration's hybrid split). */
+int mfp_row_length_quantile(uint32_t rows, const uint32_t *row_ptr, double q, uint32_t *width);
+
+/* scoo_matrix_class<T> — common/scoo_matrix_class.cpp:13-139.
+ * Parameters from (rows, sm_count, shared_mem_size, sizeof(T)) exactly as the
+ * reference computes them; slices_ptr has slices_count+1 entries and the ones
+ * after the last real slice stay 0 (value-initialised in the reference). */
+typedef struct mfp_scoo_params {
+  uint32_t slices_count;
+  uint32_t slice_size;
+  uint32_t lane_size;
+} mfp_scoo_params;
+int mfp_scoo_params_compute(uint32_t rows, uint32_t sm_count, uint64_t shared_mem_size,
+                            int value_type, mfp_scoo_params *out);
+int mfp_scoo_from_csr_f32(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                          const float *data, const mfp_scoo_params *params, float *values,
+                          uint32_t *c_index, uint32_t *r_index, uint32_t *slices_ptr);
+int mfp_scoo_from_csr_f64(uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                          const double *data, const mfp_scoo_params *params, double *values,
+                          uint32_t *c_index, uint32_t *r_index, uint32_t *slices_ptr);
+
+/* fill_row_blocks — gpu/csr_adaptive_spmv.cu:180-240, with NNZ_PER_WG as a
+ * parameter (the reference fixes it at 64).  row_blocks may be NULL to count
+ * only; otherwise it receives count+1 boundaries. */
+int mfp_csr_adaptive_row_blocks(uint32_t rows, const uint32_t *row_ptr, uint32_t nnz_per_wg,
+                                uint32_t *row_blocks, uint32_t *count);
+
+/* ------------------------------------------------------------------------- */
+/* Device-pointer SpMV entry points: y = A * x, enqueued on `stream`.        */
+/* ------------------------------------------------------------------------- */
+
+/* CSR family.  A plan partitions the rows once per sparsity pattern (long-row
+ * pieces, CSR-Adaptive row bins) and owns the scratch the pieces combine in.
+ * algo: 0 = CSR scalar (one thread per row; csr_spmv_kernel,
+ * gpu_matrix_multiplier.cu:22-43), 1 = CSR vector (a lane group per row;
+ * csr_spmv_vector_kernel, :331-362), 2 = CSR-Adaptive (row bins;
+ * csr_adaptive_spmv.cu:26-178).  Rows longer than long_row_threshold are
+ * split across CTAs; rows longer than 4096 accumulate in FP64. */
+typedef enum mfp_csr_algo { MFP_CSR_SCALAR = 0, MFP_CSR_VECTOR = 1, MFP_CSR_ADAPTIVE = 2 } mfp_csr_algo;
+typedef struct mfp_csr_config {
+  uint32_t long_row_threshold; /* 0 = default for the algo; UINT32_MAX = never split */
+  uint32_t vector_lanes;       /* CSR vector lanes per row: 2..32 (power of two); 0 = auto */
+  uint32_t bin_nnz;            /* CSR-Adaptive elements per row bin; 0 = default */
+  uint32_t piece_nnz;          /* elements per long-row piece; 0 = default (4096) */
+  uint32_t assist_threshold;   /* scalar/vector: rows longer than this (and not long) are
+                                  reduced by a whole warp; 0 = default (64);
+                                  UINT32_MAX = never (keeps the reference summation order) */
+} mfp_csr_config;
+typedef struct mfp_csr_plan mfp_csr_plan;
+int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *host_row_ptr,
+                        int algo, const mfp_csr_config *config, mfp_csr_plan **plan);
+int mfp_csr_plan_destroy(mfp_csr_plan *plan);
+/* Reads back the resolved configuration (defaults filled in). */
+int mfp_csr_plan_get_config(const mfp_csr_plan *plan, int *algo, mfp_csr_config *config,
+                            uint32_t *long_rows, uint32_t *pieces);
+/* Counterparts of gpu_csr_spmv / gpu_csr_vector_spmv / gpu_csr_adaptive_spmv
+ * (gpu_matrix_multiplier.cu:54-133, :364-447; csr_adaptive_spmv.cu:242-321)
+ * minus the per-call copies: the arrays are already on the device. */
+int mfp_csr_spmv_f32(const mfp_csr_plan *plan, const float *data, const uint32_t *col_ids,
+                     const uint32_t *row_ptr, const float *x, float *y, void *stream);
+int mfp_csr_spmv_f64(const mfp_csr_plan *plan, const double *data, const uint32_t *col_ids,
+                     const uint32_t *row_ptr, const double *x, double *y, void *stream);
+
+/* ELL — counterpart of gpu_ell_spmv (gpu_matrix_multiplier.cu:450-550). */
+int mfp_ell_spmv_f32(uint32_t rows, uint32_t cols, uint32_t width, const float *data,
+                     const uint32_t *col_ids, const float *x, float *y, void *stream);
+int mfp_ell_spmv_f64(uint32_t rows, uint32_t cols, uint32_t width, const double *data,
+                     const uint32_t *col_ids, const double *x, double *y, void *stream);
+
+/* COO — counterpart of gpu_coo_spmv (gpu_matrix_multiplier.cu:622-716).
+ * Rows must be sorted (the coo_matrix_class layout).  A segmented reduction
+ * replaces the per-element atomics: rows shared by two tiles are combined
+ * through `workspace` (device memory of mfp_coo_workspace_bytes bytes,
+ * zero-filled once before its first use; every call leaves it zeroed again).
+ * Calls that share a workspace must not overlap on the GPU. */
+int mfp_coo_workspace_bytes(uint32_t rows, uint32_t nnz, size_t *bytes);
+int mfp_coo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
+                     const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
+                     void *workspace, size_t workspace_bytes, void *stream);
+int mfp_coo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t nnz, const double *data,
+                     const uint32_t *col_ids, const uint32_t *row_ids, const double *x, double *y,
+                     void *workspace, size_t workspace_bytes, void *stream);
+/* Reads the workspace's error word (non-zero: a bounded wait gave up). Synchronous. */
+int mfp_workspace_error(const void *workspace, uint32_t *error);
+
+/* SCOO — counterpart of gpu_scoo_spmv (gpu/scoo_spmv.cu:46-222).  One CTA per
+ * slice.  x_windows (device, 2 uint32 per slice: first and one-past-last
+ * column of the slice, from mfp_scoo_x_windows) lets a slice stage its x
+ * window in shared memory when the window holds at most max_window elements;
+ * wider slices, or x_windows == NULL, gather x from global memory. */
+int mfp_scoo_x_windows(uint32_t nnz, const uint32_t *c_index, const uint32_t *slices_ptr,
+                       uint32_t slices_count, uint32_t *windows);
+int mfp_scoo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
+                      const float *values, const uint32_t *c_index, const uint32_t *r_index,
+                      const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
+                      const float *x, float *y, void *stream);
+int mfp_scoo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
+                      const double *values, const uint32_t *c_index, const uint32_t *r_index,
+                      const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
+                      const double *x, double *y, void *stream);
+
+/* Hybrid ELL + COO — counterpart of gpu_hybrid_spmv / gpu_hybrid_atomic_spmv
+ * (gpu_matrix_multiplier.cu:866-1096).  One kernel: each CTA owns
+ * MFP_HYB_ROWS_PER_BLOCK rows, adds their ELL slots and their COO-tail
+ * elements, and writes each y once (no atomics).  tail_block_ptr (device,
+ * ceil(rows / MFP_HYB_ROWS_PER_BLOCK) + 1 entries) is the first tail element
+ * of each row block, from mfp_hybrid_tail_block_ptr on the host tail rows. */
+#define MFP_HYB_ROWS_PER_BLOCK 1024u
+int mfp_hybrid_tail_block_ptr(uint32_t rows, uint32_t coo_nnz, const uint32_t *coo_rows,
+                              uint32_t *tail_block_ptr);
+int mfp_hybrid_spmv_f32(uint32_t rows, uint32_t cols, uint32_t ell_width, const float *ell_data,
+                        const uint32_t *ell_cols, uint32_t coo_nnz, const float *coo_data,
+                        const uint32_t *coo_cols, const uint32_t *coo_rows,
+                        const uint32_t *tail_block_ptr, const float *x, float *y, void *stream);
+int mfp_hybrid_spmv_f64(uint32_t rows, uint32_t cols, uint32_t ell_width, const double *ell_data,
+                        const uint32_t *ell_cols, uint32_t coo_nnz, const double *coo_data,
+                        const uint32_t *coo_cols, const uint32_t *coo_rows,
+                        const uint32_t *tail_block_ptr, const double *x, double *y,
+                        void *stream);
+
+/* fill_vector — gpu_matrix_multiplier.cu:45-52. */
+int mfp_fill_f32(uint64_t n, float *vec, float value, void *stream);
+int mfp_fill_f64(uint64_t n, double *vec, double value, void *stream);
+
+/* ------------------------------------------------------------------------- */
+/* Device-resident matrices (the reference-facing call with host x and y).   */
+/* ------------------------------------------------------------------------- */
+
+/* A handle uploads one format once and keeps it on the device with whatever
+ * plan / workspace / staging the format needs.  It replaces the caller-held
+ * resizable_gpu_memory buffers of the reference (gpu/resizable_gpu_memory.h:13-44)
+ * and the per-call H2D copies of every gpu_*_spmv wrapper. */
+typedef enum mfp_format {
+  MFP_FORMAT_CSR_SCALAR = 0,
+  MFP_FORMAT_CSR_VECTOR = 1,
+  MFP_FORMAT_CSR_ADAPTIVE = 2,
+  MFP_FORMAT_ELL = 3,
+  MFP_FORMAT_COO = 4,
+  MFP_FORMAT_SCOO = 5,
+  MFP_FORMAT_HYBRID = 6
+} mfp_format;
+typedef struct mfp_matrix mfp_matrix;
+
+/* CSR algorithms (format 0..2) from host CSR arrays. */
+int mfp_matrix_create_csr(int format, int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
+                          const uint32_t *row_ptr, const uint32_t *columns, const void *data,
+                          const mfp_csr_config *config, mfp_matrix **out);
+int mfp_matrix_create_ell(int value_type, uint32_t rows, uint32_t cols, uint32_t width,
+                          const uint32_t *ell_columns, const void *ell_data, mfp_matrix **out);
+int mfp_matrix_create_coo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
+                          const uint32_t *coo_rows, const uint32_t *coo_cols,
+                          const void *coo_data, mfp_matrix **out);
+int mfp_matrix_create_scoo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
+                           const mfp_scoo_params *params, const uint32_t *c_index,
+                           const uint32_t *r_index, const uint32_t *slices_ptr,
+                           const void *values, mfp_matrix **out);
+int mfp_matrix_create_hybrid(int value_type, uint32_t rows, uint32_t cols, uint32_t ell_width,
+                             const uint32_t *ell_columns, const void *ell_data, uint32_t coo_nnz,
+                             const uint32_t *coo_rows, const uint32_t *coo_cols,
+                             const void *coo_data, mfp_matrix **out);
+int mfp_matrix_destroy(mfp_matrix *m);
+
+typedef struct mfp_matrix_info {
+  int format;
+  int value_type;
+  uint32_t rows, cols;
+  uint64_t nnz;                /* stored non-zeros of the source matrix */
+  uint64_t format_bytes;       /* bytes one SpMV must move in this layout */
+  uint64_t algorithmic_bytes;  /* nnz*(val+4) + (rows+1)*4 + cols*val + rows*val */
+  uint64_t device_bytes;       /* device memory held by the handle */
+  uint32_t kernel_launches;    /* kernels one mfp_matrix_spmv enqueues */
+} mfp_matrix_info;
+int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out);
+
+/* y = A*x with device x and y (value type of the matrix), enqueued on stream. */
+int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream);
+/* y = A*x with HOST x and y: copies x in, runs the kernel, copies y out, and
+ * waits for the copy.  Page-locked host buffers give full PCIe bandwidth. */
+int mfp_matrix_spmv_host(mfp_matrix *m, const void *host_x, void *host_y, void *stream);
+
+/* ------------------------------------------------------------------------- */
+/* Measurement records — measurement_class (common/measurement_class.h:11-58) */
+/* and compare_results (:60-89).                                              */
+/* ------------------------------------------------------------------------- */
+typedef struct mfp_measurement {
+  char format[64];
+  double elapsed;                  /* seconds */
+  double effective_bandwidth;      /* load_store_bytes / (elapsed * 1e9) */
+  double computational_throughput; /* operations_count / (elapsed * 1e9) */
+} mfp_measurement;
+int mfp_measurement_make(const char *format, double elapsed, double load_store_bytes,
+                         double operations_count, mfp_measurement *out);
+/* Relative squared L2 error sum((a-b)^2) / sum(b^2), accumulated in T as the
+ * reference does.  *first_bad = first i with |a-b| > 1e-8 when error > 1e-9,
+ * else UINT32_MAX.  Does not print. */
+int mfp_compare_results_f32(uint32_t n, const float *a, const float *b, double *error,
+                            uint32_t *first_bad);
+int mfp_compare_results_f64(uint32_t n, const double *a, const double *b, double *error,
+                            uint32_t *first_bad);
+
+/* Times `reps` launches of mfp_matrix_spmv with CUDA events on `stream`,
+ * writing over an L2-sized buffer between launches when flush_l2 != 0.
+ * Returns the mean seconds per launch and the median. */
+int mfp_matrix_time(const mfp_matrix *m, const void *x, void *y, uint32_t reps, int flush_l2,
+                    void *stream, double *mean_seconds, double *median_seconds);
+
+/* ------------------------------------------------------------------------- */
+/* Seeded synthetic matrices (stand-ins for the SuiteSparse inputs).          */
+/* Output is CSR with sorted columns and double values; call with NULL       */
+/* arrays first to get rows and nnz.                                          */
+/* ------------------------------------------------------------------------- */
+typedef enum mfp_synth_kind {
+  MFP_SYNTH_LAPLACIAN_2D = 0, /* n x n grid, 5-point, 4 / -1 */
+  MFP_SYNTH_POWER_LAW = 1,    /* Zipf(alpha) row lengths clipped to [1, max_row] */
+  MFP_SYNTH_STENCIL_27 = 2,   /* n^3 grid, 27-point, values U[-1,1] */
+  MFP_SYNTH_BANDED = 3,       /* n rows, half bandwidth b, k distinct columns per row */
+  MFP_SYNTH_UNIFORM = 4,      /* k_lo..k_hi uniform row lengths, uniform columns */
+  MFP_SYNTH_TRIDIAGONAL = 5,
+  MFP_SYNTH_BLOCK_DIAGONAL = 6 /* dense b x b blocks on the diagonal */
+} mfp_synth_kind;
+typedef struct mfp_synth_params {
+  int kind;
+  uint64_t seed;
+  uint32_t n;       /* grid side (laplacian, stencil) or rows (others) */
+  uint32_t cols;    /* columns (power law, uniform); 0 = n */
+  double alpha;     /* Zipf exponent */
+  uint32_t k_lo, k_hi; /* row length bounds (power-law clip [k_lo, k_hi]; uniform) */
+  uint32_t band;    /* half bandwidth (banded) or block size (block diagonal) */
+} mfp_synth_params;
+int mfp_synth_csr(const mfp_synth_params *p, uint32_t *rows, uint32_t *cols, uint64_t *nnz,
+                  uint32_t *row_ptr, uint32_t *columns, double *values);
+/* Seeded uniform[lo, hi) vectors (x of every configuration). */
+int mfp_synth_vector_f64(uint64_t seed, uint64_t n, double lo, double hi, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFP_SPMV_H */

@@ -1,0 +1,104 @@
+"""Builds the engine's shared library (sm_100a CUDA kernels + C ABI) in-tree.
+
+    python -m matrix_format_performance_b200.build [--force] [--jobs N]
+
+Outputs matrix_format_performance_b200/lib/libmfp_spmv.so.  Objects go to
+matrix_format_performance_b200/_build/.  nvcc cross-compiles for sm_100a, so
+this runs on a machine without a GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libmfp_spmv.so"
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["capi.cu"]
+CPP_SOURCES = ["util.cpp", "formats.cpp", "synth.cpp"]
+HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "host_common.h"]
+
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3",
+                     "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]
+CXX_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall", "-Wextra",
+             "-Wno-unused-parameter", f"-I{CUDA_HOME / 'include'}", f"-I{ROOT / 'include'}"]
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if r.stderr.strip():
+        sys.stderr.write(r.stderr)
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "mfp_spmv.h"]
+    tasks = []
+    objs = []
+    for src in CU_SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + headers):
+            tasks.append([NVCC] + NVCC_FLAGS + ["-c", str(s), "-o", str(o)])
+    for src in CPP_SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + headers):
+            tasks.append(["g++"] + CXX_FLAGS + ["-c", str(s), "-o", str(o)])
+    with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        for f in [ex.submit(_run, t) for t in tasks]:
+            f.result()
+    if force or tasks or _stale(LIB, objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
+             + ["-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+        os.replace(tmp, LIB)
+    if verbose:
+        print(f"built {LIB}")
+    return LIB
+
+
+def clean() -> None:
+    shutil.rmtree(BUILD, ignore_errors=True)
+    if LIB.exists():
+        LIB.unlink()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("--clean", action="store_true")
+    a = ap.parse_args()
+    if a.clean:
+        clean()
+        return
+    build(force=a.force, jobs=a.jobs, verbose=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,806 @@
+// C ABI: plans, kernel launches, device-resident matrix handles and timing.
+#include "host_common.h"
+#include "spmv_kernels.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+using namespace mfp;
+namespace d = mfp::dev;
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(MFP_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+#define CUDA_TRY(expr, what)                    \
+  do {                                          \
+    cudaError_t _e = (expr);                    \
+    if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+int check_launch(const char *what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  return ok();
+}
+
+template <typename T>
+int dmalloc(T **p, size_t count, size_t *acct = nullptr) {
+  *p = nullptr;
+  if (count == 0) return MFP_SUCCESS;
+  const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? MFP_ERROR_OUT_OF_MEMORY : MFP_ERROR_CUDA,
+                "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+  }
+  if (acct) *acct += count * sizeof(T);
+  return MFP_SUCCESS;
+}
+template <typename T>
+int upload(T **p, const T *host, size_t count, size_t *acct = nullptr) {
+  int st = dmalloc(p, count, acct);
+  if (st) return st;
+  if (count) CUDA_TRY(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  return MFP_SUCCESS;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// CSR plan
+// ---------------------------------------------------------------------------
+struct mfp_csr_plan {
+  int device = 0;
+  int algo = 0;
+  mfp_csr_config cfg{};
+  uint32_t assist_thr = 64;
+  uint32_t rows = 0, cols = 0, nnz = 0;
+  uint32_t n_main = 0, n_pieces = 0, n_long = 0;
+  d::long_piece *pieces = nullptr;
+  double *partials = nullptr;
+  uint32_t *counters = nullptr;
+  uint32_t *row_blocks = nullptr;
+  size_t device_bytes = 0;
+};
+
+namespace {
+constexpr uint32_t kDefaultLong = 4096;
+constexpr uint32_t kDefaultAssist = 64;
+constexpr uint32_t kDefaultPiece = 4096;
+constexpr uint32_t kFp64Rows = 4096;  // rows longer than this accumulate in FP64
+constexpr uint32_t kMaxBin = d::kChunk - 4;
+}  // namespace
+
+extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
+                                   int algo, const mfp_csr_config *config, mfp_csr_plan **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "plan output is NULL");
+  *out = nullptr;
+  if (algo < 0 || algo > 2) return fail(MFP_ERROR_INVALID_VALUE, "unknown CSR algorithm %d", algo);
+  int st = check_row_ptr(rows, nnz, rp);
+  if (st) return st;
+  mfp_csr_config cfg = config ? *config : mfp_csr_config{};
+  auto *plan = new mfp_csr_plan();
+  cudaGetDevice(&plan->device);
+  plan->algo = algo;
+  plan->rows = rows;
+  plan->cols = cols;
+  plan->nnz = nnz;
+  if (cfg.piece_nnz == 0) cfg.piece_nnz = kDefaultPiece;
+  cfg.piece_nnz = std::max(cfg.piece_nnz, 256u);
+  if (algo == MFP_CSR_ADAPTIVE) {
+    cfg.bin_nnz = cfg.bin_nnz ? std::min(cfg.bin_nnz, kMaxBin) : kMaxBin;
+    if (cfg.long_row_threshold == 0) cfg.long_row_threshold = cfg.bin_nnz;
+  } else {
+    if (cfg.long_row_threshold == 0) cfg.long_row_threshold = kDefaultLong;
+  }
+  if (algo == MFP_CSR_VECTOR) {
+    uint32_t L = cfg.vector_lanes;
+    if (L == 0) {
+      const double mean = rows ? (double)nnz / rows : 1.0;
+      L = 2;
+      while (L * 2 <= mean && L < 32) L *= 2;
+    }
+    if (L < 2 || L > 32 || (L & (L - 1))) {
+      delete plan;
+      return fail(MFP_ERROR_INVALID_VALUE, "vector_lanes must be a power of two in [2, 32]");
+    }
+    cfg.vector_lanes = L;
+  }
+  plan->assist_thr = cfg.assist_threshold ? cfg.assist_threshold : kDefaultAssist;
+  plan->cfg = cfg;
+
+  // long rows -> pieces of at most piece_nnz elements
+  std::vector<d::long_piece> pieces;
+  uint32_t slots = 0, nlong = 0;
+  for (uint32_t r = 0; r < rows; ++r) {
+    const uint32_t len = rp[r + 1] - rp[r];
+    if (len <= cfg.long_row_threshold) continue;
+    const uint32_t np = ceil_div(len, cfg.piece_nnz);
+    for (uint32_t k = 0; k < np; ++k) {
+      d::long_piece pc{};
+      pc.row = r;
+      pc.e0 = rp[r] + k * cfg.piece_nnz;
+      pc.e1 = std::min(rp[r + 1], pc.e0 + cfg.piece_nnz);
+      pc.slot_base = slots;
+      pc.piece = k;
+      pc.npieces = np;
+      pc.counter = nlong;
+      pc.fp64 = len > kFp64Rows ? 1u : 0u;
+      pieces.push_back(pc);
+    }
+    if (np > 1) slots += np;
+    ++nlong;
+  }
+  std::vector<uint32_t> blocks;
+  if (algo == MFP_CSR_ADAPTIVE) {
+    blocks.push_back(0);
+    uint32_t cur_rows = 0, cur_nnz = 0;
+    const uint32_t max_rows = 4 * d::kBlock;
+    for (uint32_t r = 0; r < rows; ++r) {
+      const uint32_t len = rp[r + 1] - rp[r];
+      const bool own = len > cfg.long_row_threshold || len > cfg.bin_nnz;
+      if (cur_rows && (own || cur_nnz + len > cfg.bin_nnz || cur_rows >= max_rows)) {
+        blocks.push_back(r);
+        cur_rows = cur_nnz = 0;
+      }
+      if (own) {
+        blocks.push_back(r + 1);
+        continue;
+      }
+      cur_rows++;
+      cur_nnz += len;
+    }
+    if (cur_rows) blocks.push_back(rows);
+    plan->n_main = (uint32_t)blocks.size() - 1;
+  } else if (algo == MFP_CSR_SCALAR) {
+    plan->n_main = ceil_div(rows, d::kBlock);
+  } else {
+    plan->n_main = ceil_div(rows, d::kBlock);
+  }
+  plan->n_pieces = (uint32_t)pieces.size();
+  plan->n_long = nlong;
+  if ((uint64_t)plan->n_main + plan->n_pieces > 0x7fffffffull) {
+    delete plan;
+    return fail(MFP_ERROR_TOO_LARGE, "grid too large");
+  }
+  if ((st = upload(&plan->pieces, pieces.data(), pieces.size(), &plan->device_bytes)) ||
+      (st = dmalloc(&plan->partials, slots, &plan->device_bytes)) ||
+      (st = dmalloc(&plan->counters, nlong, &plan->device_bytes)) ||
+      (st = upload(&plan->row_blocks, blocks.data(), blocks.size(), &plan->device_bytes))) {
+    mfp_csr_plan_destroy(plan);
+    return st;
+  }
+  if (nlong) {
+    const cudaError_t e = cudaMemset(plan->counters, 0, nlong * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+      mfp_csr_plan_destroy(plan);
+      return cuda_fail(e, "cudaMemset counters");
+    }
+  }
+  *out = plan;
+  return ok();
+}
+
+extern "C" int mfp_csr_plan_destroy(mfp_csr_plan *plan) {
+  if (!plan) return ok();
+  cudaFree(plan->pieces);
+  cudaFree(plan->partials);
+  cudaFree(plan->counters);
+  cudaFree(plan->row_blocks);
+  delete plan;
+  return ok();
+}
+
+extern "C" int mfp_csr_plan_get_config(const mfp_csr_plan *plan, int *algo, mfp_csr_config *cfg,
+                                       uint32_t *long_rows, uint32_t *pieces) {
+  if (!plan) return fail(MFP_ERROR_INVALID_VALUE, "plan is NULL");
+  if (algo) *algo = plan->algo;
+  if (cfg) {
+    *cfg = plan->cfg;
+    cfg->assist_threshold = plan->assist_thr;
+  }
+  if (long_rows) *long_rows = plan->n_long;
+  if (pieces) *pieces = plan->n_pieces;
+  return ok();
+}
+
+namespace {
+template <typename T>
+int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, const uint32_t *rp, const T *x,
+             T *y, void *stream) {
+  if (!plan) return fail(MFP_ERROR_INVALID_VALUE, "plan is NULL");
+  if (plan->rows == 0) return ok();
+  if (!rp || !y || (plan->nnz && (!data || !cols || !x))) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  d::csr_args<T> A{};
+  A.n_rows = plan->rows;
+  A.row_ptr = rp;
+  A.cols = cols;
+  A.vals = data;
+  A.x = x;
+  A.y = y;
+  A.long_thr = plan->cfg.long_row_threshold;
+  A.assist_thr = plan->assist_thr;
+  A.lanes = plan->cfg.vector_lanes ? plan->cfg.vector_lanes : 32;
+  A.row_blocks = plan->row_blocks;
+  A.n_main = plan->n_main;
+  A.pieces = plan->pieces;
+  A.partials = plan->partials;
+  A.counters = plan->counters;
+  const bool vec = aligned16(data) && aligned16(cols);
+  const uint32_t grid = plan->n_main + plan->n_pieces;
+  if (grid == 0) return ok();
+  cudaStream_t s = as_stream(stream);
+#define MFP_CSR_LAUNCH(ALGO)                                                         \
+  if (vec)                                                                           \
+    d::csr_kernel<T, ALGO, true><<<grid, d::kBlock, 0, s>>>(A);                      \
+  else                                                                               \
+    d::csr_kernel<T, ALGO, false><<<grid, d::kBlock, 0, s>>>(A);
+  switch (plan->algo) {
+    case 0: MFP_CSR_LAUNCH(0) break;
+    case 1: MFP_CSR_LAUNCH(1) break;
+    default: MFP_CSR_LAUNCH(2) break;
+  }
+#undef MFP_CSR_LAUNCH
+  return check_launch("csr_kernel launch");
+}
+
+template <typename T>
+int ell_spmv(uint32_t rows, uint32_t width, const T *data, const uint32_t *cols, const T *x, T *y,
+             void *stream) {
+  if (rows == 0) return ok();
+  if (!y || (width && (!data || !cols || !x))) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  const bool vec = (rows % 4 == 0) && aligned16(data) && aligned16(cols) && aligned16(y);
+  cudaStream_t s = as_stream(stream);
+  if (vec)
+    d::ell_kernel<T, true><<<ceil_div(rows / 4, d::kBlock), d::kBlock, 0, s>>>(rows, width, data, cols, x, y);
+  else
+    d::ell_kernel<T, false><<<ceil_div(rows, d::kBlock), d::kBlock, 0, s>>>(rows, width, data, cols, x, y);
+  return check_launch("ell_kernel launch");
+}
+
+template <typename T>
+int fill(uint64_t n, T *v, T value, void *stream) {
+  if (n == 0) return ok();
+  if (!v) return fail(MFP_ERROR_INVALID_VALUE, "null vector");
+  const uint32_t grid = (uint32_t)std::min<uint64_t>(ceil_div(n, 512), 148u * 16u);
+  d::fill_kernel<T><<<grid, 512, 0, as_stream(stream)>>>(n, v, value);
+  return check_launch("fill_kernel launch");
+}
+
+size_t coo_ws_bytes(uint32_t nnz) {
+  const uint64_t tiles = (nnz + (uint64_t)d::kChunk - 1) / d::kChunk;
+  return sizeof(d::coo_ws_header) + tiles * sizeof(d::coo_tile_state<double>);
+}
+
+template <typename T>
+int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
+             const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
+  if (rows == 0) return ok();
+  if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
+  if (nnz == 0) return fill<T>(rows, y, T(0), stream);
+  if (!data || !cols || !rids || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  if (!ws || ws_bytes < coo_ws_bytes(nnz))
+    return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_ws_bytes(nnz), ws_bytes);
+  if (!aligned16(ws)) return fail(MFP_ERROR_INVALID_VALUE, "COO workspace must be 16-byte aligned");
+  auto *hdr = reinterpret_cast<d::coo_ws_header *>(ws);
+  auto *tiles = reinterpret_cast<d::coo_tile_state<T> *>(hdr + 1);
+  const uint32_t grid = ceil_div(nnz, d::kChunk);
+  const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
+  cudaStream_t s = as_stream(stream);
+  if (vec)
+    d::coo_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+  else
+    d::coo_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+  return check_launch("coo_kernel launch");
+}
+
+template <typename T, bool VEC, bool XWIN>
+int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32_t slice, const T *v,
+                const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
+                const T *x, T *y) {
+  auto k = d::scoo_kernel<T, VEC, XWIN>;
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024 - (int)sizeof(d::scoo_smem_static<T>));
+  });
+  k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, x, y);
+  return check_launch("scoo_kernel launch");
+}
+
+template <typename T>
+int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const uint32_t *ci,
+              const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const T *x, T *y,
+              void *stream) {
+  if (rows == 0) return ok();
+  if (!y || !sp || !v || !ci || !ri || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  if (slice == 0 || (uint64_t)slice * slices < rows) return fail(MFP_ERROR_INVALID_VALUE, "slices do not cover the rows");
+  const size_t acc_bytes = (size_t)((slice + 3u) & ~3u) * sizeof(T);
+  if (win == nullptr) maxw = 0;
+  const size_t dyn = acc_bytes + (size_t)maxw * sizeof(T);
+  if (dyn + sizeof(d::scoo_smem_static<T>) > 227 * 1024)
+    return fail(MFP_ERROR_NOT_SUPPORTED, "slice_size %u / window %u too large for shared memory", slice, maxw);
+  const bool vec = aligned16(v) && aligned16(ci) && aligned16(ri);
+  cudaStream_t s = as_stream(stream);
+  if (vec) {
+    if (win) return scoo_launch<T, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
+    return scoo_launch<T, true, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
+  }
+  if (win) return scoo_launch<T, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
+  return scoo_launch<T, false, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
+}
+
+template <typename T>
+int hyb_spmv(uint32_t rows, uint32_t width, const T *ed, const uint32_t *ec, uint32_t cnnz, const T *cd,
+             const uint32_t *cc, const uint32_t *cr, const uint32_t *tp, const T *x, T *y, void *stream) {
+  if (rows == 0) return ok();
+  if (!y || !x || !tp || (width && (!ed || !ec)) || (cnnz && (!cd || !cc || !cr)))
+    return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  const bool vec = (rows % 4 == 0) && aligned16(ed) && aligned16(ec) && aligned16(cd) && aligned16(cc) && aligned16(cr);
+  const uint32_t grid = ceil_div(rows, d::kHybRows);
+  cudaStream_t s = as_stream(stream);
+  if (vec)
+    d::hyb_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, width, ed, ec, cd, cc, cr, tp, x, y);
+  else
+    d::hyb_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, width, ed, ec, cd, cc, cr, tp, x, y);
+  return check_launch("hyb_kernel launch");
+}
+}  // namespace
+
+extern "C" {
+
+int mfp_get_device_info(int device, mfp_device_info *out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  cudaDeviceProp p{};
+  CUDA_TRY(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+  out->device = device;
+  out->sm_count = p.multiProcessorCount;
+  out->shared_mem_per_block = p.sharedMemPerBlock;
+  out->shared_mem_optin = p.sharedMemPerBlockOptin;
+  out->l2_bytes = (uint64_t)p.l2CacheSize;
+  out->global_mem_bytes = p.totalGlobalMem;
+  out->cc_major = p.major;
+  out->cc_minor = p.minor;
+  return ok();
+}
+
+int mfp_csr_spmv_f32(const mfp_csr_plan *p, const float *a, const uint32_t *c, const uint32_t *rp, const float *x,
+                     float *y, void *s) {
+  return csr_spmv<float>(p, a, c, rp, x, y, s);
+}
+int mfp_csr_spmv_f64(const mfp_csr_plan *p, const double *a, const uint32_t *c, const uint32_t *rp,
+                     const double *x, double *y, void *s) {
+  return csr_spmv<double>(p, a, c, rp, x, y, s);
+}
+int mfp_ell_spmv_f32(uint32_t rows, uint32_t, uint32_t w, const float *a, const uint32_t *c, const float *x,
+                     float *y, void *s) {
+  return ell_spmv<float>(rows, w, a, c, x, y, s);
+}
+int mfp_ell_spmv_f64(uint32_t rows, uint32_t, uint32_t w, const double *a, const uint32_t *c, const double *x,
+                     double *y, void *s) {
+  return ell_spmv<double>(rows, w, a, c, x, y, s);
+}
+int mfp_coo_workspace_bytes(uint32_t, uint32_t nnz, size_t *bytes) {
+  if (!bytes) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *bytes = coo_ws_bytes(nnz);
+  return ok();
+}
+int mfp_coo_spmv_f32(uint32_t rows, uint32_t, uint32_t nnz, const float *a, const uint32_t *c, const uint32_t *r,
+                     const float *x, float *y, void *ws, size_t wsb, void *s) {
+  return coo_spmv<float>(rows, nnz, a, c, r, x, y, ws, wsb, s);
+}
+int mfp_coo_spmv_f64(uint32_t rows, uint32_t, uint32_t nnz, const double *a, const uint32_t *c, const uint32_t *r,
+                     const double *x, double *y, void *ws, size_t wsb, void *s) {
+  return coo_spmv<double>(rows, nnz, a, c, r, x, y, ws, wsb, s);
+}
+int mfp_workspace_error(const void *ws, uint32_t *error) {
+  if (!ws || !error) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  d::coo_ws_header h{};
+  CUDA_TRY(cudaMemcpy(&h, ws, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+  *error = h.error;
+  return ok();
+}
+int mfp_scoo_spmv_f32(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, const float *v, const uint32_t *ci,
+                      const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const float *x,
+                      float *y, void *s) {
+  return scoo_spmv<float>(rows, slices, slice, v, ci, ri, sp, win, maxw, x, y, s);
+}
+int mfp_scoo_spmv_f64(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, const double *v, const uint32_t *ci,
+                      const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const double *x,
+                      double *y, void *s) {
+  return scoo_spmv<double>(rows, slices, slice, v, ci, ri, sp, win, maxw, x, y, s);
+}
+int mfp_hybrid_spmv_f32(uint32_t rows, uint32_t, uint32_t w, const float *ed, const uint32_t *ec, uint32_t cn,
+                        const float *cd, const uint32_t *cc, const uint32_t *cr, const uint32_t *tp, const float *x,
+                        float *y, void *s) {
+  return hyb_spmv<float>(rows, w, ed, ec, cn, cd, cc, cr, tp, x, y, s);
+}
+int mfp_hybrid_spmv_f64(uint32_t rows, uint32_t, uint32_t w, const double *ed, const uint32_t *ec, uint32_t cn,
+                        const double *cd, const uint32_t *cc, const uint32_t *cr, const uint32_t *tp,
+                        const double *x, double *y, void *s) {
+  return hyb_spmv<double>(rows, w, ed, ec, cn, cd, cc, cr, tp, x, y, s);
+}
+int mfp_fill_f32(uint64_t n, float *v, float value, void *s) { return fill<float>(n, v, value, s); }
+int mfp_fill_f64(uint64_t n, double *v, double value, void *s) { return fill<double>(n, v, value, s); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Device-resident matrices
+// ---------------------------------------------------------------------------
+struct mfp_matrix {
+  int format = 0, value_type = 0, device = 0;
+  uint32_t rows = 0, cols = 0;
+  uint64_t nnz = 0;
+  std::vector<void *> allocs;
+  size_t device_bytes = 0;
+  uint64_t format_bytes = 0;
+  // arrays (meaning per format)
+  void *vals = nullptr;
+  uint32_t *cols_a = nullptr;
+  uint32_t *rows_a = nullptr;   // CSR row_ptr, COO/SCOO row ids
+  uint32_t *aux = nullptr;      // SCOO slices_ptr, HYB tail block ptr
+  uint32_t *win = nullptr;      // SCOO x windows
+  void *vals2 = nullptr;        // HYB COO tail
+  uint32_t *cols2 = nullptr, *rows2 = nullptr;
+  uint32_t width = 0, coo_nnz = 0, slices = 0, slice_size = 0, max_window = 0;
+  mfp_csr_plan *plan = nullptr;
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  void *dx = nullptr, *dy = nullptr;  // staging for the host-buffer call
+};
+
+namespace {
+
+template <typename T>
+int track(mfp_matrix *m, T **p, size_t count) {
+  int st = dmalloc(p, count, &m->device_bytes);
+  if (!st && *p) m->allocs.push_back(*p);
+  return st;
+}
+template <typename T>
+int track_upload(mfp_matrix *m, T **p, const T *host, size_t count) {
+  int st = track(m, p, count);
+  if (st) return st;
+  if (count) CUDA_TRY(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  return MFP_SUCCESS;
+}
+int track_upload_bytes(mfp_matrix *m, void **p, const void *host, size_t bytes) {
+  unsigned char *q = nullptr;
+  int st = track_upload(m, &q, static_cast<const unsigned char *>(host), bytes);
+  *p = q;
+  return st;
+}
+int finish_matrix(mfp_matrix *m, mfp_matrix **out) {
+  const size_t vs = value_size(m->value_type);
+  int st = track_upload_bytes(m, &m->dx, nullptr, 0);
+  unsigned char *a = nullptr, *b = nullptr;
+  if (!st) st = track(m, &a, (size_t)std::max(1u, m->cols) * vs);
+  if (!st) st = track(m, &b, (size_t)std::max(1u, m->rows) * vs);
+  m->dx = a;
+  m->dy = b;
+  if (st) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  *out = m;
+  return ok();
+}
+bool valid_vt(int vt) { return vt == MFP_F32 || vt == MFP_F64; }
+
+}  // namespace
+
+extern "C" {
+
+int mfp_matrix_destroy(mfp_matrix *m) {
+  if (!m) return ok();
+  for (void *p : m->allocs) cudaFree(p);
+  mfp_csr_plan_destroy(m->plan);
+  delete m;
+  return ok();
+}
+
+int mfp_matrix_create_csr(int format, int vt, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
+                          const uint32_t *ci, const void *data, const mfp_csr_config *cfg, mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (format < 0 || format > 2 || !valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad format or value type");
+  if (nnz && (!ci || !data)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  int st = check_row_ptr(rows, nnz, rp);
+  if (st) return st;
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = format;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  const size_t vs = value_size(vt);
+  m->format_bytes = (uint64_t)nnz * (vs + 4) + ((uint64_t)rows + 1) * 4 + (uint64_t)cols * vs + (uint64_t)rows * vs;
+  if ((st = track_upload_bytes(m, &m->vals, data, (size_t)nnz * vs)) ||
+      (st = track_upload(m, &m->cols_a, ci, nnz)) || (st = track_upload(m, &m->rows_a, rp, (size_t)rows + 1)) ||
+      (st = mfp_csr_plan_create(rows, cols, nnz, rp, format, cfg, &m->plan))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  m->device_bytes += m->plan->device_bytes;
+  return finish_matrix(m, out);
+}
+
+int mfp_matrix_create_ell(int vt, uint32_t rows, uint32_t cols, uint32_t width, const uint32_t *ec,
+                          const void *ed, mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
+  const uint64_t slots = (uint64_t)rows * width;
+  if (slots && (!ec || !ed)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  const size_t vs = value_size(vt);
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_ELL;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->width = width;
+  // non-padding slots: a padding slot holds column 0 and value 0
+  uint64_t nz = 0;
+  for (uint64_t i = 0; i < slots; ++i) {
+    const bool zero = vt == MFP_F64 ? static_cast<const double *>(ed)[i] == 0.0 : static_cast<const float *>(ed)[i] == 0.0f;
+    nz += !(zero && ec[i] == 0);
+  }
+  m->nnz = nz;
+  m->format_bytes = slots * (vs + 4) + (uint64_t)cols * vs + (uint64_t)rows * vs;
+  int st;
+  if ((st = track_upload_bytes(m, &m->vals, ed, slots * vs)) || (st = track_upload(m, &m->cols_a, ec, slots))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  return finish_matrix(m, out);
+}
+
+int mfp_matrix_create_coo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *cr,
+                          const uint32_t *cc, const void *cd, mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
+  if (nnz && (!cr || !cc || !cd)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  for (uint32_t i = 0; i < nnz; ++i) {
+    if (cr[i] >= rows || cc[i] >= cols) return fail(MFP_ERROR_INVALID_VALUE, "index out of range at element %u", i);
+    if (i && cr[i] < cr[i - 1]) return fail(MFP_ERROR_INVALID_VALUE, "COO rows must be sorted (element %u)", i);
+  }
+  const size_t vs = value_size(vt);
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_COO;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  m->format_bytes = (uint64_t)nnz * (vs + 8) + (uint64_t)cols * vs + (uint64_t)rows * vs;
+  m->ws_bytes = coo_ws_bytes(nnz);
+  unsigned char *ws = nullptr;
+  int st;
+  if ((st = track_upload_bytes(m, &m->vals, cd, (size_t)nnz * vs)) || (st = track_upload(m, &m->cols_a, cc, nnz)) ||
+      (st = track_upload(m, &m->rows_a, cr, nnz)) || (st = track(m, &ws, m->ws_bytes))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  m->ws = ws;
+  if (ws && cudaMemset(ws, 0, m->ws_bytes) != cudaSuccess) {
+    mfp_matrix_destroy(m);
+    return fail(MFP_ERROR_CUDA, "cudaMemset workspace");
+  }
+  return finish_matrix(m, out);
+}
+
+int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, const mfp_scoo_params *prm,
+                           const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const void *v,
+                           mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (!valid_vt(vt) || !prm || !sp) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
+  if (nnz && (!ci || !ri || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  const size_t vs = value_size(vt);
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_SCOO;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  m->slices = prm->slices_count;
+  m->slice_size = prm->slice_size;
+  m->format_bytes = (uint64_t)nnz * (vs + 8) + ((uint64_t)m->slices + 1) * 4 + (uint64_t)cols * vs + (uint64_t)rows * vs;
+  // x windows: stage a slice's x window in shared memory when most windows fit
+  std::vector<uint32_t> win(2 * (size_t)m->slices);
+  mfp_scoo_x_windows(nnz, ci, sp, m->slices, win.data());
+  std::vector<uint32_t> widths;
+  for (uint32_t s = 0; s < m->slices; ++s)
+    if (win[2 * s + 1] > win[2 * s]) widths.push_back(win[2 * s + 1] - win[2 * s]);
+  const uint32_t cap = (uint32_t)((vt == MFP_F64 ? 48u : 96u) * 1024u / vs);
+  bool use_win = false;
+  if (!widths.empty()) {
+    std::sort(widths.begin(), widths.end());
+    const uint32_t p90 = widths[(widths.size() * 9) / 10];
+    if (p90 <= cap) {
+      use_win = true;
+      m->max_window = std::min(cap, widths.back());
+      m->max_window = (m->max_window + 3u) & ~3u;
+    }
+  }
+  int st;
+  if ((st = track_upload_bytes(m, &m->vals, v, (size_t)nnz * vs)) || (st = track_upload(m, &m->cols_a, ci, nnz)) ||
+      (st = track_upload(m, &m->rows_a, ri, nnz)) || (st = track_upload(m, &m->aux, sp, (size_t)m->slices + 1)) ||
+      (use_win && (st = track_upload(m, &m->win, win.data(), win.size())))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  return finish_matrix(m, out);
+}
+
+int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t width, const uint32_t *ec,
+                             const void *ed, uint32_t cnnz, const uint32_t *cr, const uint32_t *cc, const void *cd,
+                             mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
+  const uint64_t slots = (uint64_t)rows * width;
+  if ((slots && (!ec || !ed)) || (cnnz && (!cr || !cc || !cd))) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  for (uint32_t i = 0; i < cnnz; ++i) {
+    if (cr[i] >= rows || cc[i] >= cols) return fail(MFP_ERROR_INVALID_VALUE, "tail index out of range at %u", i);
+    if (i && cr[i] < cr[i - 1]) return fail(MFP_ERROR_INVALID_VALUE, "tail rows must be sorted (element %u)", i);
+  }
+  const size_t vs = value_size(vt);
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_HYBRID;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->width = width;
+  m->coo_nnz = cnnz;
+  uint64_t nz = 0;
+  for (uint64_t i = 0; i < slots; ++i) {
+    const bool zero = vt == MFP_F64 ? static_cast<const double *>(ed)[i] == 0.0 : static_cast<const float *>(ed)[i] == 0.0f;
+    nz += !(zero && ec[i] == 0);
+  }
+  m->nnz = nz + cnnz;
+  const uint32_t nb = ceil_div(rows, MFP_HYB_ROWS_PER_BLOCK);
+  std::vector<uint32_t> tp((size_t)nb + 1);
+  mfp_hybrid_tail_block_ptr(rows, cnnz, cr, tp.data());
+  m->format_bytes = slots * (vs + 4) + (uint64_t)cnnz * (vs + 8) + ((uint64_t)nb + 1) * 4 + (uint64_t)cols * vs +
+                    (uint64_t)rows * vs;
+  int st;
+  if ((st = track_upload_bytes(m, &m->vals, ed, slots * vs)) || (st = track_upload(m, &m->cols_a, ec, slots)) ||
+      (st = track_upload_bytes(m, &m->vals2, cd, (size_t)cnnz * vs)) || (st = track_upload(m, &m->cols2, cc, cnnz)) ||
+      (st = track_upload(m, &m->rows2, cr, cnnz)) || (st = track_upload(m, &m->aux, tp.data(), tp.size()))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  return finish_matrix(m, out);
+}
+
+int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
+  if (!m || !out) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const size_t vs = value_size(m->value_type);
+  out->format = m->format;
+  out->value_type = m->value_type;
+  out->rows = m->rows;
+  out->cols = m->cols;
+  out->nnz = m->nnz;
+  out->format_bytes = m->format_bytes;
+  out->algorithmic_bytes = m->nnz * (vs + 4) + ((uint64_t)m->rows + 1) * 4 + (uint64_t)m->cols * vs + (uint64_t)m->rows * vs;
+  out->device_bytes = m->device_bytes;
+  out->kernel_launches = 1;
+  return ok();
+}
+
+int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
+  if (!m || !y || (!x && m->cols)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const bool f64 = m->value_type == MFP_F64;
+  switch (m->format) {
+    case MFP_FORMAT_CSR_SCALAR:
+    case MFP_FORMAT_CSR_VECTOR:
+    case MFP_FORMAT_CSR_ADAPTIVE:
+      return f64 ? csr_spmv<double>(m->plan, (const double *)m->vals, m->cols_a, m->rows_a, (const double *)x,
+                                    (double *)y, stream)
+                 : csr_spmv<float>(m->plan, (const float *)m->vals, m->cols_a, m->rows_a, (const float *)x,
+                                   (float *)y, stream);
+    case MFP_FORMAT_ELL:
+      return f64 ? ell_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, (const double *)x,
+                                    (double *)y, stream)
+                 : ell_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, (const float *)x,
+                                   (float *)y, stream);
+    case MFP_FORMAT_COO:
+      return f64 ? coo_spmv<double>(m->rows, (uint32_t)m->nnz, (const double *)m->vals, m->cols_a, m->rows_a,
+                                    (const double *)x, (double *)y, m->ws, m->ws_bytes, stream)
+                 : coo_spmv<float>(m->rows, (uint32_t)m->nnz, (const float *)m->vals, m->cols_a, m->rows_a,
+                                   (const float *)x, (float *)y, m->ws, m->ws_bytes, stream);
+    case MFP_FORMAT_SCOO:
+      return f64 ? scoo_spmv<double>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
+                                     m->rows_a, m->aux, m->win, m->max_window, (const double *)x, (double *)y, stream)
+                 : scoo_spmv<float>(m->rows, m->slices, m->slice_size, (const float *)m->vals, m->cols_a, m->rows_a,
+                                    m->aux, m->win, m->max_window, (const float *)x, (float *)y, stream);
+    case MFP_FORMAT_HYBRID:
+      return f64 ? hyb_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, m->coo_nnz,
+                                    (const double *)m->vals2, m->cols2, m->rows2, m->aux, (const double *)x,
+                                    (double *)y, stream)
+                 : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
+                                   (const float *)m->vals2, m->cols2, m->rows2, m->aux, (const float *)x, (float *)y,
+                                   stream);
+    default:
+      return fail(MFP_ERROR_INVALID_VALUE, "unknown format %d", m->format);
+  }
+}
+
+int mfp_matrix_spmv_host(mfp_matrix *m, const void *hx, void *hy, void *stream) {
+  if (!m || !hy || (!hx && m->cols)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const size_t vs = value_size(m->value_type);
+  cudaStream_t s = as_stream(stream);
+  if (m->cols)
+    CUDA_TRY(cudaMemcpyAsync(m->dx, hx, (size_t)m->cols * vs, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync x");
+  int st = mfp_matrix_spmv(m, m->dx, m->dy, stream);
+  if (st) return st;
+  if (m->rows)
+    CUDA_TRY(cudaMemcpyAsync(hy, m->dy, (size_t)m->rows * vs, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync y");
+  CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return ok();
+}
+
+int mfp_matrix_time(const mfp_matrix *m, const void *x, void *y, uint32_t reps, int flush_l2, void *stream,
+                    double *mean_s, double *median_s) {
+  if (!m || reps == 0) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  static void *flush_buf = nullptr;
+  static size_t flush_bytes = 0;
+  static std::mutex mu;
+  if (flush_l2) {
+    std::lock_guard<std::mutex> g(mu);
+    if (!flush_buf) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      int l2 = 0;
+      cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+      flush_bytes = (size_t)std::max(l2, 1 << 20) * 2;
+      CUDA_TRY(cudaMalloc(&flush_buf, flush_bytes), "cudaMalloc flush buffer");
+    }
+  }
+  std::vector<cudaEvent_t> ev(2 * (size_t)reps);
+  for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e), "cudaEventCreate");
+  int st = MFP_SUCCESS;
+  for (uint32_t i = 0; i < reps && !st; ++i) {
+    if (flush_l2) cudaMemsetAsync(flush_buf, (int)(i & 0xff), flush_bytes, s);
+    cudaEventRecord(ev[2 * i], s);
+    st = mfp_matrix_spmv(m, x, y, stream);
+    cudaEventRecord(ev[2 * i + 1], s);
+  }
+  std::vector<double> t;
+  if (!st) {
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamSynchronize");
+  }
+  if (!st)
+    for (uint32_t i = 0; i < reps; ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+      t.push_back(ms * 1e-3);
+    }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (st) return st;
+  double sum = 0;
+  for (double v : t) sum += v;
+  std::sort(t.begin(), t.end());
+  if (mean_s) *mean_s = sum / reps;
+  if (median_s) *median_s = t[t.size() / 2];
+  return ok();
+}
+
+}  // extern "C"

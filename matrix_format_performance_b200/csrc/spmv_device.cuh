@@ -1,0 +1,311 @@
+// Device helpers shared by every SpMV format kernel (sm_100a).
+//
+// SpMV moves ~6-12 bytes per multiply-add, so every kernel here is bound by
+// HBM bandwidth and by the L2 gathers of x.  The helpers encode the three
+// rules all kernels follow:
+//  1. matrix arrays (values, column ids, row ids) are read exactly once:
+//     16-byte vector loads, L1 no-allocate, L2 evict-first, so they do not
+//     push x out of L1/L2;
+//  2. x is gathered through the read-only path (L1-cached, normal L2 priority);
+//  3. products are formed with an explicitly rounded multiply and summed with
+//     an explicitly rounded add (no FMA contraction), so a row summed in CSR
+//     order gives exactly the result of the reference CPU loop
+//     (cpu/cpu_matrix_multiplier.cpp:34-43), not merely a close one.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mfp {
+namespace dev {
+
+constexpr int kWarp = 32;
+
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// ---- streaming loads -------------------------------------------------------
+__device__ __forceinline__ void ld_stream4(const float *p, float (&v)[4], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+               : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream4(const double *p, double (&v)[4], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
+               : "=d"(v[0]), "=d"(v[1])
+               : "l"(p), "l"(pol));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
+               : "=d"(v[2]), "=d"(v[3])
+               : "l"(p + 2), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream4(const uint32_t *p, uint32_t (&v)[4], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ float ld_stream1(const float *p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+               : "=f"(v)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_stream1(const double *p, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
+               : "=d"(v)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream1(const uint32_t *p, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+               : "=r"(v)
+               : "l"(p), "l"(pol));
+  return v;
+}
+
+// x gathers: read-only path, cached in L1.
+template <typename T>
+__device__ __forceinline__ T ld_x(const T *p) {
+  return __ldg(p);
+}
+
+// ---- arithmetic without contraction ---------------------------------------
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// Neumaier-compensated double accumulator (used for rows longer than 4096
+// elements and for combining long-row partial sums).
+struct comp_sum {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double v) {
+    const double t = __dadd_rn(s, v);
+    if (fabs(s) >= fabs(v))
+      c = __dadd_rn(c, __dadd_rn(__dsub_rn(s, t), v));
+    else
+      c = __dadd_rn(c, __dadd_rn(__dsub_rn(v, t), s));
+    s = t;
+  }
+  __device__ __forceinline__ void add(const comp_sum &o) {
+    add(o.s);
+    c = __dadd_rn(c, o.c);
+  }
+  __device__ __forceinline__ double value() const { return __dadd_rn(s, c); }
+};
+
+// ---- reductions ------------------------------------------------------------
+// Tree over lane offsets width/2 .. 1 with shuffle-down, the same tree as the
+// reference warp_reduce (gpu/reduce.cuh:6-20) when width == 32; the result is
+// in the first lane of each group.
+template <typename T>
+__device__ __forceinline__ T group_reduce_down(T v, int width) {
+  for (int off = width >> 1; off > 0; off >>= 1) v = add_rn(v, __shfl_down_sync(0xffffffffu, v, off, width));
+  return v;
+}
+
+template <typename T, int BLOCK>
+__device__ __forceinline__ T block_reduce(T v, T *s_scratch /* >= BLOCK/32 */) {
+  v = group_reduce_down(v, kWarp);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_scratch[warp] = v;
+  __syncthreads();
+  T r = T(0);
+  if (warp == 0) {
+    r = lane < BLOCK / 32 ? s_scratch[lane] : T(0);
+    r = group_reduce_down(r, kWarp);
+  }
+  return r;  // valid in thread 0
+}
+
+template <int BLOCK>
+__device__ __forceinline__ comp_sum block_reduce_comp(comp_sum v, double *s_s, double *s_c) {
+  for (int off = 16; off > 0; off >>= 1) {
+    comp_sum o;
+    o.s = __shfl_down_sync(0xffffffffu, v.s, off);
+    o.c = __shfl_down_sync(0xffffffffu, v.c, off);
+    v.add(o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    s_s[warp] = v.s;
+    s_c[warp] = v.c;
+  }
+  __syncthreads();
+  comp_sum r;
+  if (warp == 0) {
+    if (lane < BLOCK / 32) {
+      r.s = s_s[lane];
+      r.c = s_c[lane];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      comp_sum o;
+      o.s = __shfl_down_sync(0xffffffffu, r.s, off);
+      o.c = __shfl_down_sync(0xffffffffu, r.c, off);
+      r.add(o);
+    }
+  }
+  return r;  // valid in thread 0
+}
+
+// Exclusive block scan of small unsigned counts (one per thread).
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp /* BLOCK/32+1 */,
+                                                         uint32_t *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, inc, off);
+    if (lane >= off) inc += o;
+  }
+  __syncthreads();
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < BLOCK / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, wi, off);
+      if (lane >= off) wi += o;
+    }
+    if (lane < BLOCK / 32) s_warp[lane] = wi - w;
+    if (lane == BLOCK / 32 - 1) s_warp[BLOCK / 32] = wi;
+  }
+  __syncthreads();
+  *total = s_warp[BLOCK / 32];
+  return s_warp[warp] + inc - v;
+}
+
+// ---- staging ---------------------------------------------------------------
+// Writes p[e] = vals[e] * x[cols[e]] for e in [a, b) to dst[e - (a & ~3)].
+// The matrix arrays are read with 16-byte loads on 4-element groups (VEC) and
+// the products are stored as whole groups, so shared-memory stores are 16- or
+// 32-byte wide and conflict-free.  dst must hold b - (a & ~3) elements.
+template <typename T, int BLOCK, bool VEC>
+__device__ __forceinline__ void stage_products(const T *__restrict__ vals,
+                                               const uint32_t *__restrict__ cols,
+                                               const T *__restrict__ x, uint32_t a, uint32_t b,
+                                               T *__restrict__ dst, uint64_t pol) {
+  const uint32_t base = a & ~3u;
+  if (VEC) {
+    const uint32_t a4 = (a + 3u) & ~3u;
+    const uint32_t b4 = b & ~3u;
+    if (a4 < b4) {
+      // head [a, a4), body [a4, b4), tail [b4, b)
+      if (threadIdx.x < a4 - a) {
+        const uint32_t e = a + threadIdx.x;
+        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+      }
+      if (threadIdx.x < b - b4) {
+        const uint32_t e = b4 + threadIdx.x;
+        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+      }
+      const uint32_t ng = (b4 - a4) >> 2;
+      uint32_t g = threadIdx.x;
+      for (; g + BLOCK < ng; g += 2 * BLOCK) {
+        const uint32_t e0 = a4 + 4u * g, e1 = e0 + 4u * BLOCK;
+        T v0[4], v1[4];
+        uint32_t c0[4], c1[4];
+        ld_stream4(vals + e0, v0, pol);
+        ld_stream4(cols + e0, c0, pol);
+        ld_stream4(vals + e1, v1, pol);
+        ld_stream4(cols + e1, c1, pol);
+        T p0[4], p1[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p0[k] = mul_rn(v0[k], ld_x(x + c0[k]));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p1[k] = mul_rn(v1[k], ld_x(x + c1[k]));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[e0 - base + k] = p0[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[e1 - base + k] = p1[k];
+      }
+      if (g < ng) {
+        const uint32_t e0 = a4 + 4u * g;
+        T v0[4];
+        uint32_t c0[4];
+        ld_stream4(vals + e0, v0, pol);
+        ld_stream4(cols + e0, c0, pol);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[e0 - base + k] = mul_rn(v0[k], ld_x(x + c0[k]));
+      }
+      return;
+    }
+  }
+  for (uint32_t e = a + threadIdx.x; e < b; e += BLOCK)
+    dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+}
+
+// Same, also staging the row id of every element (COO-like layouts).
+template <typename T, int BLOCK, bool VEC>
+__device__ __forceinline__ void stage_products_rows(const T *__restrict__ vals,
+                                                    const uint32_t *__restrict__ cols,
+                                                    const uint32_t *__restrict__ rows,
+                                                    const T *__restrict__ x, uint32_t a, uint32_t b,
+                                                    T *__restrict__ dst, uint32_t *__restrict__ dst_rows,
+                                                    uint64_t pol) {
+  const uint32_t base = a & ~3u;
+  if (VEC) {
+    const uint32_t a4 = (a + 3u) & ~3u;
+    const uint32_t b4 = b & ~3u;
+    if (a4 < b4) {
+      if (threadIdx.x < a4 - a) {
+        const uint32_t e = a + threadIdx.x;
+        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+        dst_rows[e - base] = ld_stream1(rows + e, pol);
+      }
+      if (threadIdx.x < b - b4) {
+        const uint32_t e = b4 + threadIdx.x;
+        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+        dst_rows[e - base] = ld_stream1(rows + e, pol);
+      }
+      const uint32_t ng = (b4 - a4) >> 2;
+      for (uint32_t g = threadIdx.x; g < ng; g += BLOCK) {
+        const uint32_t e0 = a4 + 4u * g;
+        T v0[4];
+        uint32_t c0[4], r0[4];
+        ld_stream4(vals + e0, v0, pol);
+        ld_stream4(cols + e0, c0, pol);
+        ld_stream4(rows + e0, r0, pol);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          dst[e0 - base + k] = mul_rn(v0[k], ld_x(x + c0[k]));
+          dst_rows[e0 - base + k] = r0[k];
+        }
+      }
+      return;
+    }
+  }
+  for (uint32_t e = a + threadIdx.x; e < b; e += BLOCK) {
+    dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+    dst_rows[e - base] = ld_stream1(rows + e, pol);
+  }
+}
+
+// Bounded spin on a flag written by an earlier CTA of the same launch.
+// Returns false (and the caller records an error) if the limit is reached.
+__device__ __forceinline__ bool wait_flag(const uint32_t *flag, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    if (v != 0u) return true;
+    __nanosleep(64);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void store_release(uint32_t *flag, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
+}
+
+}  // namespace dev
+}  // namespace mfp

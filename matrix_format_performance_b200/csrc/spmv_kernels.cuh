@@ -1,0 +1,905 @@
+// SpMV format kernels for B200 (sm_100a).
+//
+// Every kernel stages a CTA's share of the matrix through shared memory as
+// products p = value * x[col] (16-byte streaming loads, see spmv_device.cuh)
+// and then reduces the products by row.  What differs per format is how
+// rows are assigned to threads, which mirrors the reference algorithm of the
+// same name:
+//   CSR scalar    one thread sums one row, in CSR order
+//                 (gpu/gpu_matrix_multiplier.cu:22-43)
+//   CSR vector    a group of 2..32 lanes per row, lane-strided + shuffle tree
+//                 (gpu/gpu_matrix_multiplier.cu:331-362, gpu/reduce.cuh)
+//   CSR-Adaptive  host-built row bins; many-row bins reduce from shared
+//                 memory, single-row bins by the whole CTA
+//                 (gpu/csr_adaptive_spmv.cu:26-178)
+//   ELL           one thread per row over column-major slots
+//                 (gpu/gpu_matrix_multiplier.cu:450-471)
+//   COO           tiles of consecutive elements, block segmented reduction,
+//                 rows shared by tiles combined by look-back
+//                 (replaces the atomics of gpu_matrix_multiplier.cu:622-638)
+//   SCOO          one CTA per slice, shared-memory row accumulators and an
+//                 optional shared-memory copy of the slice's x window
+//                 (gpu/scoo_spmv.cu:46-129)
+//   HYB           one CTA per row block: ELL slots plus the block's COO tail
+//                 (gpu/gpu_matrix_multiplier.cu:969-1002)
+// Rows longer than a plan threshold (CSR family) are cut into pieces that
+// run as extra CTAs of the same launch and meet in a partial-sum buffer.
+#pragma once
+
+#include "spmv_device.cuh"
+
+namespace mfp {
+namespace dev {
+
+constexpr int kBlock = 256;   // threads per CTA for every kernel
+constexpr int kEpt = 8;       // staged elements per thread
+constexpr int kChunk = kBlock * kEpt;  // elements staged per phase
+constexpr int kChunkPad = kChunk + 64; // room for the alignment offset and swizzle
+
+// Shared-memory swizzle: XOR the low 5 bits of an index with bits 5..9.
+// Rows walked one element at a time by consecutive threads (stride = row
+// length) and per-thread contiguous ranges (stride 8) both hit 32 banks.
+__device__ __forceinline__ uint32_t swz(uint32_t i) { return i ^ ((i >> 5) & 31u); }
+
+// Store elements i..i+3 (i a multiple of 4) of a swizzled array with one
+// 16-byte (float) or two 16-byte (double) stores.
+template <typename T>
+__device__ __forceinline__ void store_group4(T *dst, uint32_t i, const T (&v)[4]);
+template <>
+__device__ __forceinline__ void store_group4<float>(float *dst, uint32_t i, const float (&v)[4]) {
+  const uint32_t s = (i >> 5) & 31u, m = s & 3u;
+  const float a0 = (m & 1u) ? v[1] : v[0], a1 = (m & 1u) ? v[0] : v[1];
+  const float a2 = (m & 1u) ? v[3] : v[2], a3 = (m & 1u) ? v[2] : v[3];
+  float4 w;
+  w.x = (m & 2u) ? a2 : a0;
+  w.y = (m & 2u) ? a3 : a1;
+  w.z = (m & 2u) ? a0 : a2;
+  w.w = (m & 2u) ? a1 : a3;
+  *reinterpret_cast<float4 *>(dst + (i ^ (s & ~3u))) = w;
+}
+template <>
+__device__ __forceinline__ void store_group4<double>(double *dst, uint32_t i, const double (&v)[4]) {
+  const uint32_t s = (i >> 5) & 31u, m = s & 3u;
+  const double a0 = (m & 1u) ? v[1] : v[0], a1 = (m & 1u) ? v[0] : v[1];
+  const double a2 = (m & 1u) ? v[3] : v[2], a3 = (m & 1u) ? v[2] : v[3];
+  double2 w0, w1;
+  w0.x = (m & 2u) ? a2 : a0;
+  w0.y = (m & 2u) ? a3 : a1;
+  w1.x = (m & 2u) ? a0 : a2;
+  w1.y = (m & 2u) ? a1 : a3;
+  double *g = dst + (i ^ (s & ~3u));
+  reinterpret_cast<double2 *>(g)[0] = w0;
+  reinterpret_cast<double2 *>(g)[1] = w1;
+}
+template <typename T>
+__device__ __forceinline__ void store_group4_u32(uint32_t *dst, uint32_t i, const uint32_t (&v)[4]) {
+  const uint32_t s = (i >> 5) & 31u, m = s & 3u;
+  const uint32_t a0 = (m & 1u) ? v[1] : v[0], a1 = (m & 1u) ? v[0] : v[1];
+  const uint32_t a2 = (m & 1u) ? v[3] : v[2], a3 = (m & 1u) ? v[2] : v[3];
+  uint4 w;
+  w.x = (m & 2u) ? a2 : a0;
+  w.y = (m & 2u) ? a3 : a1;
+  w.z = (m & 2u) ? a0 : a2;
+  w.w = (m & 2u) ? a1 : a3;
+  *reinterpret_cast<uint4 *>(dst + (i ^ (s & ~3u))) = w;
+}
+
+// x source: global memory, or a shared-memory window [lo, lo + n).
+template <typename T>
+struct x_global {
+  const T *__restrict__ x;
+  __device__ __forceinline__ T operator()(uint32_t c) const { return ld_x(x + c); }
+};
+template <typename T>
+struct x_window {
+  const T *s_x;
+  uint32_t lo;
+  __device__ __forceinline__ T operator()(uint32_t c) const { return s_x[c - lo]; }
+};
+
+// Stage products of elements [a, b) (b - (a & ~3) <= kChunkPad - 32) into
+// dst at swizzled local index e - (a & ~3); optionally also their row ids.
+template <typename T, bool VEC, bool ROWS, typename XS>
+__device__ __forceinline__ void stage(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                      const uint32_t *__restrict__ rows, XS xs, uint32_t a,
+                                      uint32_t b, T *__restrict__ dst, uint32_t *__restrict__ dst_rows,
+                                      uint64_t pol) {
+  const uint32_t base = a & ~3u;
+  uint32_t s0 = a, s1 = b;  // scalar part(s)
+  if (VEC) {
+    const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
+    if (a4 < b4) {
+      if (threadIdx.x < a4 - a) {
+        const uint32_t e = a + threadIdx.x;
+        dst[swz(e - base)] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+        if (ROWS) dst_rows[swz(e - base)] = ld_stream1(rows + e, pol);
+      }
+      if (threadIdx.x < b - b4) {
+        const uint32_t e = b4 + threadIdx.x;
+        dst[swz(e - base)] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+        if (ROWS) dst_rows[swz(e - base)] = ld_stream1(rows + e, pol);
+      }
+      const uint32_t ng = (b4 - a4) >> 2;
+      uint32_t g = threadIdx.x;
+      for (; g + kBlock < ng; g += 2 * kBlock) {
+        const uint32_t e0 = a4 + 4u * g, e1 = e0 + 4u * kBlock;
+        T v0[4], v1[4];
+        uint32_t c0[4], c1[4], r0[4], r1[4];
+        ld_stream4(vals + e0, v0, pol);
+        ld_stream4(cols + e0, c0, pol);
+        ld_stream4(vals + e1, v1, pol);
+        ld_stream4(cols + e1, c1, pol);
+        if (ROWS) {
+          ld_stream4(rows + e0, r0, pol);
+          ld_stream4(rows + e1, r1, pol);
+        }
+        T p0[4], p1[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p0[k] = mul_rn(v0[k], xs(c0[k]));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p1[k] = mul_rn(v1[k], xs(c1[k]));
+        store_group4<T>(dst, e0 - base, p0);
+        store_group4<T>(dst, e1 - base, p1);
+        if (ROWS) {
+          store_group4_u32<T>(dst_rows, e0 - base, r0);
+          store_group4_u32<T>(dst_rows, e1 - base, r1);
+        }
+      }
+      if (g < ng) {
+        const uint32_t e0 = a4 + 4u * g;
+        T v0[4];
+        uint32_t c0[4], r0[4];
+        ld_stream4(vals + e0, v0, pol);
+        ld_stream4(cols + e0, c0, pol);
+        if (ROWS) ld_stream4(rows + e0, r0, pol);
+        T p0[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p0[k] = mul_rn(v0[k], xs(c0[k]));
+        store_group4<T>(dst, e0 - base, p0);
+        if (ROWS) store_group4_u32<T>(dst_rows, e0 - base, r0);
+      }
+      return;
+    }
+  }
+  for (uint32_t e = s0 + threadIdx.x; e < s1; e += kBlock) {
+    dst[swz(e - base)] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+    if (ROWS) dst_rows[swz(e - base)] = ld_stream1(rows + e, pol);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block segmented reduction over staged (product, row) pairs.
+// Local indices [off, off + n), n <= kChunk, off < 4, rows non-decreasing.
+// Thread t owns [off + t*kEpt, off + (t+1)*kEpt).  Calls
+//   emit(row, total, is_first_segment, is_last_segment)
+// exactly once per row present in the chunk, from one thread, and
+//   gap(lo, hi) for every run of absent rows lo..hi-1 strictly between two
+// present rows.  Sums are deterministic (fixed order for a given chunking).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct seg_scan_smem {
+  T warp_v[kBlock / 32];
+  uint32_t warp_f[kBlock / 32];
+  T prefix_v[kBlock / 32];
+  uint32_t prefix_f[kBlock / 32];
+};
+
+template <typename T, typename Emit, typename Gap>
+__device__ __forceinline__ void block_segmented_reduce(const T *s_prod, const uint32_t *s_row,
+                                                       uint32_t off, uint32_t n, Emit emit, Gap gap,
+                                                       seg_scan_smem<T> &sm) {
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t end = off + n;
+  const uint32_t i0 = off + t * kEpt;
+  const uint32_t i1 = min(i0 + kEpt, end);
+  const bool active = i0 < end;
+  const uint32_t row_first_chunk = s_row[swz(off)];
+  const uint32_t row_last_chunk = s_row[swz(end - 1)];
+
+  uint32_t first_row = 0, last_row = 0;
+  T first_sum = T(0), cur = T(0);
+  bool multi = false, head_cont = false;
+  if (active) {
+    first_row = s_row[swz(i0)];
+    if (i0 > off) {
+      const uint32_t prev = s_row[swz(i0 - 1)];
+      head_cont = (prev == first_row);
+      if (!head_cont && first_row > prev + 1u) gap(prev + 1u, first_row);
+    }
+    uint32_t r = first_row;
+    cur = s_prod[swz(i0)];
+    for (uint32_t i = i0 + 1; i < i1; ++i) {
+      const uint32_t ri = s_row[swz(i)];
+      const T p = s_prod[swz(i)];
+      if (ri != r) {
+        if (!multi) {
+          first_sum = cur;
+          multi = true;
+        } else {
+          emit(r, cur, false, false);
+        }
+        if (ri > r + 1u) gap(r + 1u, ri);
+        r = ri;
+        cur = p;
+      } else {
+        cur = add_rn(cur, p);
+      }
+    }
+    last_row = r;
+  }
+  // Segmented inclusive scan of the last-run partials across threads.  A
+  // thread continues its left neighbour's chain only if it holds a single run
+  // of the row that the neighbour's last run has.
+  uint32_t f = (active && !multi && head_cont) ? 0u : 1u;
+  T v = active ? cur : T(0);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T ov = __shfl_up_sync(0xffffffffu, v, o);
+    const uint32_t of = __shfl_up_sync(0xffffffffu, f, o);
+    if (lane >= (uint32_t)o) {
+      if (!f) v = add_rn(ov, v);
+      f |= of;
+    }
+  }
+  if (lane == 31) {
+    sm.warp_v[warp] = v;
+    sm.warp_f[warp] = f;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // exclusive prefix over warps (kBlock/32 <= 32 entries)
+    const uint32_t nw = kBlock / 32;
+    T wv = lane < nw ? sm.warp_v[lane] : T(0);
+    uint32_t wf = lane < nw ? sm.warp_f[lane] : 1u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T ov = __shfl_up_sync(0xffffffffu, wv, o);
+      const uint32_t of = __shfl_up_sync(0xffffffffu, wf, o);
+      if (lane >= (uint32_t)o) {
+        if (!wf) wv = add_rn(ov, wv);
+        wf |= of;
+      }
+    }
+    // inclusive (wv, wf) at lane w -> exclusive for warp w+1
+    const T pv = __shfl_up_sync(0xffffffffu, wv, 1);
+    const uint32_t pf = __shfl_up_sync(0xffffffffu, wf, 1);
+    if (lane < nw) {
+      sm.prefix_v[lane] = lane == 0 ? T(0) : pv;
+      sm.prefix_f[lane] = lane == 0 ? 1u : pf;
+    }
+  }
+  __syncthreads();
+  if (!f && warp > 0) v = add_rn(sm.prefix_v[warp], v);  // chain reaches into previous warps
+  // S_{t-1}
+  T left = __shfl_up_sync(0xffffffffu, v, 1);
+  if (lane == 0) left = warp > 0 ? sm.prefix_v[warp] : T(0);
+
+  if (!active) return;
+  const bool tail_cont = (i1 < end) && (s_row[swz(i1)] == last_row);
+  if (multi) {
+    if (head_cont)
+      emit(first_row, add_rn(left, first_sum), first_row == row_first_chunk, first_row == row_last_chunk);
+    else
+      emit(first_row, first_sum, first_row == row_first_chunk, first_row == row_last_chunk);
+    if (!tail_cont) emit(last_row, cur, false, last_row == row_last_chunk);
+  } else if (!tail_cont) {
+    emit(last_row, v, last_row == row_first_chunk, last_row == row_last_chunk);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Long-row pieces (CSR family)
+// ---------------------------------------------------------------------------
+struct long_piece {
+  uint32_t row;
+  uint32_t e0, e1;     // element range of this piece
+  uint32_t slot_base;  // first partial slot of the row (pieces of a row are consecutive)
+  uint32_t piece;      // index of this piece within the row
+  uint32_t npieces;
+  uint32_t counter;    // arrival counter of the row
+  uint32_t fp64;       // 1: accumulate in FP64 (rows longer than 4096)
+};
+
+template <typename T, bool VEC>
+__device__ __forceinline__ void run_piece(const long_piece &pc, const T *__restrict__ vals,
+                                          const uint32_t *__restrict__ cols, const T *__restrict__ x,
+                                          T *__restrict__ y, double *partials, uint32_t *counters,
+                                          double *s_a, double *s_b, uint64_t pol) {
+  const uint32_t a = pc.e0, b = pc.e1;
+  double result;
+  if (pc.fp64) {
+    comp_sum acc;
+    uint32_t s0 = a, s1 = b;
+    if (VEC) {
+      const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
+      if (a4 < b4) {
+        const uint32_t ng = (b4 - a4) >> 2;
+        for (uint32_t g = threadIdx.x; g < ng; g += kBlock) {
+          const uint32_t e0 = a4 + 4u * g;
+          T v[4];
+          uint32_t c[4];
+          ld_stream4(vals + e0, v, pol);
+          ld_stream4(cols + e0, c, pol);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc.add(__dmul_rn((double)v[k], (double)ld_x(x + c[k])));
+        }
+        if (threadIdx.x < a4 - a) {
+          const uint32_t e = a + threadIdx.x;
+          acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
+        }
+        if (threadIdx.x < b - b4) {
+          const uint32_t e = b4 + threadIdx.x;
+          acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
+        }
+        s0 = s1 = 0;
+      }
+    }
+    for (uint32_t e = s0 + threadIdx.x; e < s1; e += kBlock)
+      acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
+    const comp_sum r = block_reduce_comp<kBlock>(acc, s_a, s_b);
+    result = r.value();
+  } else {
+    T acc = T(0);
+    uint32_t s0 = a, s1 = b;
+    if (VEC) {
+      const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
+      if (a4 < b4) {
+        const uint32_t ng = (b4 - a4) >> 2;
+        for (uint32_t g = threadIdx.x; g < ng; g += kBlock) {
+          const uint32_t e0 = a4 + 4u * g;
+          T v[4];
+          uint32_t c[4];
+          ld_stream4(vals + e0, v, pol);
+          ld_stream4(cols + e0, c, pol);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc = add_rn(acc, mul_rn(v[k], ld_x(x + c[k])));
+        }
+        if (threadIdx.x < a4 - a) {
+          const uint32_t e = a + threadIdx.x;
+          acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
+        }
+        if (threadIdx.x < b - b4) {
+          const uint32_t e = b4 + threadIdx.x;
+          acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
+        }
+        s0 = s1 = 0;
+      }
+    }
+    for (uint32_t e = s0 + threadIdx.x; e < s1; e += kBlock)
+      acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
+    result = (double)block_reduce<T, kBlock>(acc, reinterpret_cast<T *>(s_a));
+  }
+  if (threadIdx.x != 0) return;
+  if (pc.npieces == 1) {
+    y[pc.row] = (T)result;
+    return;
+  }
+  partials[pc.slot_base + pc.piece] = result;
+  __threadfence();
+  const uint32_t arrived = atomicAdd(counters + pc.counter, 1u);
+  if (arrived == pc.npieces - 1) {
+    __threadfence();
+    comp_sum s;
+    for (uint32_t k = 0; k < pc.npieces; ++k) s.add(__ldcg(partials + pc.slot_base + k));
+    y[pc.row] = (T)s.value();
+    counters[pc.counter] = 0u;  // ready for the next launch
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CSR family kernel: blocks [0, n_main) run the algorithm's main part,
+// blocks [n_main, n_main + n_pieces) run long-row pieces.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct csr_args {
+  uint32_t n_rows;
+  const uint32_t *__restrict__ row_ptr;
+  const uint32_t *__restrict__ cols;
+  const T *__restrict__ vals;
+  const T *__restrict__ x;
+  T *__restrict__ y;
+  uint32_t long_thr;    // rows with more elements are handled by pieces
+  uint32_t assist_thr;  // scalar/vector: rows with more elements are reduced by a warp
+  uint32_t lanes;       // CSR vector: lanes per row (power of two, 2..32)
+  const uint32_t *__restrict__ row_blocks;  // CSR-Adaptive bins (n_main + 1 entries)
+  uint32_t n_main;
+  const long_piece *__restrict__ pieces;
+  double *partials;
+  uint32_t *counters;
+};
+
+template <typename T>
+struct csr_smem {
+  union {
+    struct {
+      uint32_t rp[kBlock + 1];
+      uint32_t longs[kBlock];
+      uint32_t assists[kBlock];
+      uint32_t nlong, nassist;
+      uint32_t wc[kBlock / 32];
+      T acc[kBlock];
+      __align__(16) T prod[kChunkPad];
+    } m;
+    struct {
+      double a[kBlock / 32];
+      double b[kBlock / 32];
+    } p;
+  };
+};
+
+// Ordered compaction of the threads whose flag is set; returns the count.
+template <typename T>
+__device__ __forceinline__ uint32_t compact_ordered(bool flag, uint32_t value, uint32_t *list,
+                                                    csr_smem<T> &sm, uint32_t *count_slot) {
+  const uint32_t t = threadIdx.x;
+  const uint32_t ballot = __ballot_sync(0xffffffffu, flag);
+  if ((t & 31u) == 0) sm.m.wc[t >> 5] = __popc(ballot);
+  __syncthreads();
+  if (t == 0) {
+    uint32_t s = 0;
+    for (int w = 0; w < kBlock / 32; ++w) {
+      const uint32_t c = sm.m.wc[w];
+      sm.m.wc[w] = s;
+      s += c;
+    }
+    *count_slot = s;
+  }
+  __syncthreads();
+  if (flag) list[sm.m.wc[t >> 5] + __popc(ballot & ((1u << (t & 31u)) - 1u))] = value;
+  __syncthreads();
+  return *count_slot;
+}
+
+// CSR scalar (MODE 0) and CSR vector (MODE 1) share the row-block skeleton:
+// CTA b owns rows [b*256, b*256+256); the elements of its rows, minus rows
+// above the long threshold, are staged in chunks; then
+//   scalar: thread t adds the products of row t one by one in CSR order;
+//   vector: row j is reduced by lane group j % (256/L), lane l taking the
+//           elements rs + l + k*L, then a shuffle tree over the group;
+// and in both, rows above the assist threshold are reduced by a warp.
+template <typename T, int MODE, bool VEC>
+__device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol) {
+  const uint32_t r0 = blockIdx.x * kBlock;
+  const uint32_t nr = min((uint32_t)kBlock, A.n_rows - r0);
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  for (uint32_t i = t; i <= nr; i += kBlock) sm.m.rp[i] = A.row_ptr[r0 + i];
+  if (t < kBlock) sm.m.acc[t] = T(0);
+  __syncthreads();
+  const bool has = t < nr;
+  const uint32_t rs = has ? sm.m.rp[t] : 0u, re = has ? sm.m.rp[t + 1] : 0u;
+  const bool is_long = has && (re - rs > A.long_thr);
+  const bool is_assist = has && !is_long && (re - rs > A.assist_thr);
+  const uint32_t nlong = compact_ordered<T>(is_long, t, sm.m.longs, sm, &sm.m.nlong);
+  const uint32_t nassist = compact_ordered<T>(is_assist, t, sm.m.assists, sm, &sm.m.nassist);
+  const uint32_t L = (MODE == 1) ? A.lanes : 1u;
+  T acc = T(0);  // scalar: running sum of this thread's row
+  uint32_t run_lo = 0;
+  for (uint32_t k = 0; k <= nlong; ++k) {
+    const uint32_t run_hi = k < nlong ? sm.m.longs[k] : nr;
+    if (run_lo < run_hi) {
+      const uint32_t a = sm.m.rp[run_lo], b = sm.m.rp[run_hi];
+      for (uint32_t c0 = a; c0 < b;) {
+        const uint32_t base = c0 & ~3u;
+        const uint32_t c1 = min(b, base + (uint32_t)kChunk);
+        stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, c0, c1, sm.m.prod, nullptr, pol);
+        __syncthreads();
+        if (MODE == 0) {
+          if (has && !is_long && !is_assist && t >= run_lo && t < run_hi) {
+            const uint32_t lo = max(rs, c0), hi = min(re, c1);
+            for (uint32_t e = lo; e < hi; ++e) acc = add_rn(acc, sm.m.prod[swz(e - base)]);
+          }
+        } else {
+          const uint32_t G = kBlock / L, g = t / L, gl = t % L;
+          for (uint32_t it = 0; it < L; ++it) {
+            const uint32_t j = g + it * G;
+            T part = T(0);
+            bool valid = false;
+            if (j < nr && j >= run_lo && j < run_hi) {
+              const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
+              const uint32_t len = je - js;
+              if (len <= A.assist_thr) {
+                const uint32_t s = max(js, c0), e = min(je, c1);
+                if (s < e) {
+                  valid = true;
+                  for (uint32_t i = s + ((gl - (s - js)) & (L - 1u)); i < e; i += L)
+                    part = add_rn(part, sm.m.prod[swz(i - base)]);
+                }
+              }
+            }
+            part = group_reduce_down(part, (int)L);
+            if (valid && gl == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
+          }
+        }
+        // rows above the assist threshold: one warp per row segment
+        for (uint32_t q = warp; q < nassist; q += kBlock / 32) {
+          const uint32_t j = sm.m.assists[q];
+          const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
+          const uint32_t s = max(js, c0), e = min(je, c1);
+          if (s < e) {
+            T part = T(0);
+            for (uint32_t i = s + ((lane - (s - js)) & 31u); i < e; i += 32) part = add_rn(part, sm.m.prod[swz(i - base)]);
+            part = group_reduce_down(part, 32);
+            if (lane == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
+          }
+        }
+        __syncthreads();
+        c0 = c1;
+      }
+    }
+    run_lo = run_hi + 1;
+  }
+  if (has && !is_long) {
+    if (MODE == 0 && !is_assist)
+      A.y[r0 + t] = acc;
+    else
+      A.y[r0 + t] = sm.m.acc[t];
+  }
+}
+
+// CSR-Adaptive: bin [row_blocks[b], row_blocks[b+1]).  Many-row bins are
+// staged whole (the binning caps their elements at bin_nnz <= kChunk - 4) and
+// reduced from shared memory by power-of-two lane groups; a single-row bin is
+// reduced by the whole CTA straight from global memory; a single row above
+// the long threshold belongs to pieces.
+template <typename T, bool VEC>
+__device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol) {
+  const uint32_t rb = A.row_blocks[blockIdx.x], re = A.row_blocks[blockIdx.x + 1];
+  const uint32_t nrows = re - rb;
+  const uint32_t t = threadIdx.x;
+  if (nrows == 0) return;
+  const uint32_t a = A.row_ptr[rb], b = A.row_ptr[re];
+  if (nrows == 1) {
+    if (b - a > A.long_thr) return;
+    T acc = T(0);
+    for (uint32_t e = a + t; e < b; e += kBlock)
+      acc = add_rn(acc, mul_rn(ld_stream1(A.vals + e, pol), ld_x(A.x + ld_stream1(A.cols + e, pol))));
+    acc = block_reduce<T, kBlock>(acc, reinterpret_cast<T *>(sm.p.a));
+    if (t == 0) A.y[rb] = acc;
+    return;
+  }
+  const uint32_t base = a & ~3u;
+  for (uint32_t i = t; i <= nrows && i <= (uint32_t)kBlock; i += kBlock) sm.m.rp[i] = A.row_ptr[rb + i];
+  if (b > a) stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, a, b, sm.m.prod, nullptr, pol);
+  __syncthreads();
+  if (nrows <= (uint32_t)kBlock) {
+    uint32_t tpr = kBlock / nrows;  // >= 1
+    tpr = tpr >= 32 ? 32u : (1u << (31 - __clz(tpr)));
+    const uint32_t grp = t / tpr, lane = t % tpr;
+    T acc = T(0);
+    const bool valid = grp < nrows;
+    if (valid) {
+      const uint32_t s = sm.m.rp[grp], e = sm.m.rp[grp + 1];
+      for (uint32_t i = s + lane; i < e; i += tpr) acc = add_rn(acc, sm.m.prod[swz(i - base)]);
+    }
+    acc = group_reduce_down(acc, (int)tpr);
+    if (valid && lane == 0) A.y[rb + grp] = acc;
+  } else {
+    for (uint32_t r = t; r < nrows; r += kBlock) {
+      const uint32_t s = A.row_ptr[rb + r], e = A.row_ptr[rb + r + 1];
+      T acc = T(0);
+      for (uint32_t i = s; i < e; ++i) acc = add_rn(acc, sm.m.prod[swz(i - base)]);
+      A.y[rb + r] = acc;
+    }
+  }
+}
+
+template <typename T, int ALGO, bool VEC>
+__global__ void __launch_bounds__(kBlock) csr_kernel(const csr_args<T> A) {
+  __shared__ csr_smem<T> sm;
+  const uint64_t pol = policy_evict_first();
+  if (blockIdx.x >= A.n_main) {
+    const long_piece pc = A.pieces[blockIdx.x - A.n_main];
+    run_piece<T, VEC>(pc, A.vals, A.cols, A.x, A.y, A.partials, A.counters, sm.p.a, sm.p.b, pol);
+    return;
+  }
+  if (ALGO == 2)
+    csr_adaptive_main<T, VEC>(A, sm, pol);
+  else
+    csr_rowblock_main<T, ALGO, VEC>(A, sm, pol);
+}
+
+// ---------------------------------------------------------------------------
+// ELL: thread per 4 consecutive rows (16-byte loads per slot) or per row.
+// Sums slots in order 0..width-1 like the reference loop, padding included.
+// ---------------------------------------------------------------------------
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(kBlock) ell_kernel(uint32_t n_rows, uint32_t width,
+                                                     const T *__restrict__ data,
+                                                     const uint32_t *__restrict__ cols,
+                                                     const T *__restrict__ x, T *__restrict__ y) {
+  const uint64_t pol = policy_evict_first();
+  if (VEC) {
+    const uint32_t r = (blockIdx.x * kBlock + threadIdx.x) * 4u;
+    if (r >= n_rows) return;
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    const size_t stride = n_rows;
+    for (uint32_t k = 0; k < width; ++k) {
+      T v[4];
+      uint32_t c[4];
+      ld_stream4(data + k * stride + r, v, pol);
+      ld_stream4(cols + k * stride + r, c, pol);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[j] = add_rn(acc[j], mul_rn(v[j], ld_x(x + c[j])));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) y[r + j] = acc[j];
+  } else {
+    const uint32_t r = blockIdx.x * kBlock + threadIdx.x;
+    if (r >= n_rows) return;
+    T acc = T(0);
+    const size_t stride = n_rows;
+    for (uint32_t k = 0; k < width; ++k) {
+      const size_t o = k * stride + r;
+      acc = add_rn(acc, mul_rn(ld_stream1(data + o, pol), ld_x(x + ld_stream1(cols + o, pol))));
+    }
+    y[r] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// COO: tile = kChunk consecutive elements, taken in launch order from an
+// atomic ticket so every lower tile is already running.  Rows split between
+// tiles: the tile holding a row's last element (END) walks back over the
+// published partials of the earlier tiles (START / MIDDLE).  Waits are
+// bounded; on timeout the workspace error word is set.
+// ---------------------------------------------------------------------------
+struct coo_ws_header {
+  uint32_t ticket;
+  uint32_t done;
+  uint32_t error;
+  uint32_t pad;
+};
+template <typename T>
+struct coo_tile_state {
+  uint32_t flag;  // 1 when published
+  uint32_t kind;  // 1 START, 2 MIDDLE
+  T value;
+};
+
+constexpr uint32_t kNoRow = 0xffffffffu;
+constexpr uint32_t kWaitLimit = 1u << 22;  // ~0.3 s of 64 ns sleeps
+
+template <typename T>
+struct coo_smem {
+  __align__(16) T prod[kChunkPad];
+  __align__(16) uint32_t row[kChunkPad];
+  seg_scan_smem<T> scan;
+  uint32_t tile;
+  T first_total, last_total;
+  uint32_t first_row, last_row;
+};
+
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(kBlock) coo_kernel(uint32_t n_rows, uint32_t nnz,
+                                                     const T *__restrict__ vals,
+                                                     const uint32_t *__restrict__ cols,
+                                                     const uint32_t *__restrict__ rows,
+                                                     const T *__restrict__ x, T *__restrict__ y,
+                                                     coo_ws_header *ws, coo_tile_state<T> *tiles) {
+  __shared__ coo_smem<T> sm;
+  const uint64_t pol = policy_evict_first();
+  if (threadIdx.x == 0) sm.tile = atomicAdd(&ws->ticket, 1u);
+  __syncthreads();
+  const uint32_t tile = sm.tile;
+  const uint32_t c0 = tile * (uint32_t)kChunk;
+  const uint32_t c1 = min(nnz, c0 + (uint32_t)kChunk);
+  const uint32_t p = c0 > 0 ? rows[c0 - 1] : kNoRow;
+  const uint32_t nx = c1 < nnz ? rows[c1] : kNoRow;
+  const uint32_t base = c0 & ~3u;  // c0 is a multiple of kChunk: base == c0
+  stage<T, VEC, true>(vals, cols, rows, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
+  __syncthreads();
+  const uint32_t off = c0 - base, n = c1 - c0;
+  const uint32_t rf = sm.row[swz(off)], rl = sm.row[swz(off + n - 1)];
+  // empty rows before the first row of this tile (after the previous tile's last)
+  {
+    const uint32_t lo = (p == kNoRow) ? 0u : p + 1u;
+    for (uint32_t r = lo + threadIdx.x; r < rf && r < n_rows; r += kBlock) y[r] = T(0);
+    if (c1 == nnz)
+      for (uint32_t r = rl + 1u + threadIdx.x; r < n_rows; r += kBlock) y[r] = T(0);
+  }
+  auto emit = [&](uint32_t row, T total, bool is_first, bool is_last) {
+    const bool cont_prev = is_first && row == p;
+    const bool cont_next = is_last && row == nx;
+    if (!cont_prev && !cont_next) {
+      if (row < n_rows) y[row] = total;
+      return;
+    }
+    if (is_first) sm.first_total = total;
+    if (is_last) sm.last_total = total;
+  };
+  auto gap = [&](uint32_t lo, uint32_t hi) {
+    for (uint32_t r = lo; r < hi && r < n_rows; ++r) y[r] = T(0);
+  };
+  block_segmented_reduce<T>(sm.prod, sm.row, off, n, emit, gap, sm.scan);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const bool first_prev = (rf == p), last_next = (rl == nx);
+    if (rf == rl) {
+      const T v = sm.first_total;
+      if (first_prev && last_next) {
+        tiles[tile].value = v;
+        tiles[tile].kind = 2u;
+        __threadfence();
+        store_release(&tiles[tile].flag, 1u);
+      } else if (!first_prev && last_next) {
+        tiles[tile].value = v;
+        tiles[tile].kind = 1u;
+        __threadfence();
+        store_release(&tiles[tile].flag, 1u);
+      }
+    } else if (last_next) {
+      tiles[tile].value = sm.last_total;
+      tiles[tile].kind = 1u;
+      __threadfence();
+      store_release(&tiles[tile].flag, 1u);
+    }
+    if (first_prev && !(rf == rl && last_next)) {
+      // this tile ends row rf: walk back over earlier tiles
+      T sum = T(0);
+      uint32_t c = tile;
+      bool ok = true;
+      while (c > 0) {
+        --c;
+        if (!wait_flag(&tiles[c].flag, kWaitLimit)) {
+          ok = false;
+          break;
+        }
+        const T v = tiles[c].value;
+        const uint32_t kind = tiles[c].kind;
+        tiles[c].flag = 0u;  // consumed
+        sum = add_rn(v, sum);
+        if (kind != 2u) break;
+      }
+      if (!ok) atomicOr(&ws->error, 1u);
+      if (rf < n_rows) y[rf] = add_rn(sum, sm.first_total);
+    }
+    __threadfence();
+    const uint32_t d = atomicAdd(&ws->done, 1u);
+    if (d == gridDim.x - 1) {
+      ws->ticket = 0u;
+      ws->done = 0u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SCOO: one CTA per slice; row accumulators and (optionally) the slice's x
+// window live in dynamic shared memory.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct scoo_smem_static {
+  __align__(16) T prod[kChunkPad];
+  __align__(16) uint32_t row[kChunkPad];
+  seg_scan_smem<T> scan;
+};
+
+template <typename T, bool VEC, bool XWIN>
+__global__ void __launch_bounds__(kBlock) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
+                                                      const T *__restrict__ vals,
+                                                      const uint32_t *__restrict__ cidx,
+                                                      const uint32_t *__restrict__ ridx,
+                                                      const uint32_t *__restrict__ slices_ptr,
+                                                      const uint32_t *__restrict__ windows,
+                                                      uint32_t max_window, const T *__restrict__ x,
+                                                      T *__restrict__ y) {
+  __shared__ scoo_smem_static<T> sm;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  T *acc = reinterpret_cast<T *>(dyn);                       // slice_size (rounded to 4)
+  T *s_x = acc + ((slice_size + 3u) & ~3u);                  // max_window + 4 when XWIN
+  const uint64_t pol = policy_evict_first();
+  const uint32_t s = blockIdx.x;
+  const uint32_t row0 = s * slice_size;
+  if (row0 >= n_rows) return;
+  const uint32_t nrows = min(slice_size, n_rows - row0);
+  const uint32_t eb = slices_ptr[s], ee = slices_ptr[s + 1];
+  for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) acc[i] = T(0);
+  bool use_win = false;
+  uint32_t wlo = 0;
+  if (XWIN && eb < ee) {
+    wlo = windows[2 * s];
+    const uint32_t whi = windows[2 * s + 1];
+    if (whi > wlo && whi - wlo <= max_window) {
+      use_win = true;
+      for (uint32_t i = threadIdx.x; i < whi - wlo; i += kBlock) s_x[i] = ld_x(x + wlo + i);
+    }
+  }
+  __syncthreads();
+  auto emit = [&](uint32_t row, T total, bool, bool) {
+    const uint32_t lr = row - row0;
+    if (lr < nrows) acc[lr] = add_rn(acc[lr], total);
+  };
+  auto gap = [](uint32_t, uint32_t) {};
+  for (uint32_t c0 = eb; c0 < ee;) {
+    const uint32_t base = c0 & ~3u;
+    const uint32_t c1 = min(ee, base + (uint32_t)kChunk);
+    if (XWIN && use_win)
+      stage<T, VEC, true>(vals, cidx, ridx, x_window<T>{s_x, wlo}, c0, c1, sm.prod, sm.row, pol);
+    else
+      stage<T, VEC, true>(vals, cidx, ridx, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
+    __syncthreads();
+    block_segmented_reduce<T>(sm.prod, sm.row, c0 - base, c1 - c0, emit, gap, sm.scan);
+    __syncthreads();
+    c0 = c1;
+  }
+  for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
+}
+
+// ---------------------------------------------------------------------------
+// HYB: CTA b owns rows [b*1024, b*1024+1024): 4 rows per thread over the ELL
+// slots, then the block's COO-tail elements [tail_ptr[b], tail_ptr[b+1]).
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHybRows = 1024;
+template <typename T>
+struct hyb_smem {
+  __align__(16) T acc[kHybRows];
+  __align__(16) T prod[kChunkPad];
+  __align__(16) uint32_t row[kChunkPad];
+  seg_scan_smem<T> scan;
+};
+
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(kBlock) hyb_kernel(uint32_t n_rows, uint32_t width,
+                                                     const T *__restrict__ ell_data,
+                                                     const uint32_t *__restrict__ ell_cols,
+                                                     const T *__restrict__ coo_data,
+                                                     const uint32_t *__restrict__ coo_cols,
+                                                     const uint32_t *__restrict__ coo_rows,
+                                                     const uint32_t *__restrict__ tail_ptr,
+                                                     const T *__restrict__ x, T *__restrict__ y) {
+  __shared__ hyb_smem<T> sm;
+  const uint64_t pol = policy_evict_first();
+  const uint32_t r0 = blockIdx.x * kHybRows;
+  const uint32_t nr = min(kHybRows, n_rows - r0);
+  const size_t stride = n_rows;
+  if (VEC) {  // n_rows % 4 == 0
+    const uint32_t lr = threadIdx.x * 4u;
+    if (lr < nr) {
+      T a[4] = {T(0), T(0), T(0), T(0)};
+      for (uint32_t k = 0; k < width; ++k) {
+        T v[4];
+        uint32_t c[4];
+        ld_stream4(ell_data + k * stride + r0 + lr, v, pol);
+        ld_stream4(ell_cols + k * stride + r0 + lr, c, pol);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a[j] = add_rn(a[j], mul_rn(v[j], ld_x(x + c[j])));
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sm.acc[lr + j] = a[j];
+    }
+  } else {
+    for (uint32_t lr = threadIdx.x; lr < nr; lr += kBlock) {
+      T a = T(0);
+      for (uint32_t k = 0; k < width; ++k) {
+        const size_t o = k * stride + r0 + lr;
+        a = add_rn(a, mul_rn(ld_stream1(ell_data + o, pol), ld_x(x + ld_stream1(ell_cols + o, pol))));
+      }
+      sm.acc[lr] = a;
+    }
+  }
+  __syncthreads();
+  const uint32_t tb = tail_ptr[blockIdx.x], te = tail_ptr[blockIdx.x + 1];
+  auto emit = [&](uint32_t row, T total, bool, bool) {
+    const uint32_t lr = row - r0;
+    if (lr < nr) sm.acc[lr] = add_rn(sm.acc[lr], total);
+  };
+  auto gap = [](uint32_t, uint32_t) {};
+  for (uint32_t c0 = tb; c0 < te;) {
+    const uint32_t base = c0 & ~3u;
+    const uint32_t c1 = min(te, base + (uint32_t)kChunk);
+    stage<T, VEC, true>(coo_data, coo_cols, coo_rows, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
+    __syncthreads();
+    block_segmented_reduce<T>(sm.prod, sm.row, c0 - base, c1 - c0, emit, gap, sm.scan);
+    __syncthreads();
+    c0 = c1;
+  }
+  for (uint32_t i = threadIdx.x; i < nr; i += kBlock) y[r0 + i] = sm.acc[i];
+}
+
+template <typename T>
+__global__ void fill_kernel(uint64_t n, T *v, T value) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = value;
+}
+
+}  // namespace dev
+}  // namespace mfp

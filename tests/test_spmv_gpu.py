@@ -1,0 +1,278 @@
+"""Parity of every sm_100a format kernel with the oracle (needs a B200).
+
+Criteria
+  exact      CSR scalar (one thread per row, CSR order) and ELL (slots in
+             order) equal the reference CPU loop bit for bit; CSR vector with
+             32 lanes equals the reference's reduce-order loop for rows whose
+             elements are staged in one chunk.
+  tolerance  every format, per row: |y - y*| <= TOL * sum_j |a_ij x_j|, with
+             y* the extended-precision product of the same (rounded) inputs;
+             TOL = 1e-5 for float32 and 1e-12 for float64.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_cases, load_golden
+from matrix_format_performance_b200 import formats as F
+from matrix_format_performance_b200 import synth
+from matrix_format_performance_b200._capi import call
+from matrix_format_performance_b200.device import (COO, CSR_ADAPTIVE, CSR_SCALAR, CSR_VECTOR, ELL, HYBRID, SCOO,
+                                                   DeviceMatrix)
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.dtype(np.float32): 1e-5, np.dtype(np.float64): 1e-12}
+ALL = [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID]
+NEVER = 0xFFFFFFFF
+EXACT_SCALAR = {"long_row_threshold": NEVER, "assist_threshold": NEVER}
+EXACT_VECTOR = {"long_row_threshold": NEVER, "assist_threshold": NEVER, "vector_lanes": 32}
+
+
+def run(m, fmt, x, config=None, hybrid_width=None, reps=1):
+    dm = DeviceMatrix.build(m, fmt, config=config, hybrid_width=hybrid_width)
+    xt = torch.from_numpy(np.ascontiguousarray(x, m.dtype)).cuda()
+    outs = []
+    for _ in range(reps):
+        yt = torch.full((m.rows,), float("nan"), dtype=xt.dtype, device="cuda")
+        dm.spmv(xt, yt)
+        torch.cuda.synchronize()
+        outs.append(yt.cpu().numpy())
+    dm.close()
+    return outs if reps > 1 else outs[0]
+
+
+def check_tol(oracle_lib, m, x, y, what=""):
+    ys, ab = oracle_lib.csr_spmv_exact(m.rows, m.row_ptr, m.columns, m.data, x.astype(m.dtype))
+    err = np.abs(y.astype(np.float64) - ys)
+    bound = TOL[m.dtype] * ab
+    bad = np.nonzero(~(err <= bound))[0]
+    assert bad.size == 0, (f"{what}: {bad.size} rows out of tolerance, first {bad[:5]}, "
+                           f"err {err[bad[:5]]}, bound {bound[bad[:5]]}")
+
+
+def golden_csr(g, s):
+    dt = np.float32 if s == "f32" else np.float64
+    return F.csr_matrix_class.from_arrays(int(g["rows"][0]), int(g["cols"][0]), g[f"csr_row_ptr_{s}"],
+                                          g[f"csr_columns_{s}"], g[f"csr_data_{s}"], dt)
+
+
+def single_chunk_windows(m, block=256, chunk=2048):
+    rp = m.row_ptr.astype(np.int64)
+    for r0 in range(0, m.rows, block):
+        r1 = min(m.rows, r0 + block)
+        if rp[r1] - (rp[r0] & ~3) > chunk:
+            return False
+    return True
+
+
+@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("s", ["f32", "f64"])
+def test_exact_formats_match_reference_bits(case, s):
+    g = load_golden(case)
+    m = golden_csr(g, s)
+    x = g["x"].astype(m.dtype)
+    assert np.array_equal(run(m, CSR_SCALAR, x, EXACT_SCALAR), g[f"yx_{s}"])
+    assert np.array_equal(run(m, ELL, x), g[f"yx_{s}"])
+    yv = run(m, CSR_VECTOR, x, EXACT_VECTOR)
+    if single_chunk_windows(m):
+        assert np.array_equal(yv, g[f"yxro_{s}"])
+    ones = np.ones(m.cols, m.dtype)
+    assert np.array_equal(run(m, CSR_SCALAR, ones, EXACT_SCALAR), g[f"y1_{s}"])
+
+
+@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("s", ["f32", "f64"])
+@pytest.mark.parametrize("fmt", ALL)
+def test_all_formats_within_tolerance_on_fixtures(oracle_lib, case, s, fmt):
+    g = load_golden(case)
+    m = golden_csr(g, s)
+    x = g["x"].astype(m.dtype)
+    check_tol(oracle_lib, m, x, run(m, fmt, x), f"{case}/{s}/fmt{fmt}")
+
+
+def _synthetic():
+    return {
+        "laplacian_512": synth.laplacian_2d(512),
+        "power_law_300k": synth.power_law(rows=300_000, seed=11),
+        "stencil_40": synth.stencil_27(40, seed=2),
+        "banded_200k": synth.banded(n=200_000, seed=4),
+        "uniform_rect": synth.uniform(50_000, 0, 40, seed=9, cols=70_001),
+    }
+
+
+SYN = {}
+
+
+def syn(name):
+    if name not in SYN:
+        SYN[name] = _synthetic()[name]
+    return SYN[name]
+
+
+@pytest.mark.parametrize("name", ["laplacian_512", "power_law_300k", "stencil_40", "banded_200k", "uniform_rect"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("fmt", ALL)
+def test_synthetic_configs_within_tolerance(oracle_lib, name, dt, fmt):
+    m = syn(name).astype(dt)
+    if fmt == ELL and F.ell_matrix_class.estimate_size(m) > 50_000_000:
+        pytest.skip("ELL padding too large for this matrix (the reference skips it too)")
+    x = synth.vector(0, m.cols).astype(dt)
+    hw = F.row_length_quantile(m, 2 / 3) if fmt == HYBRID else None
+    check_tol(oracle_lib, m, x, run(m, fmt, x, hybrid_width=hw), f"{name}/{dt.__name__}/fmt{fmt}")
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_scalar_and_ell_exact_on_laplacian_512(oracle_lib, dt):
+    m = syn("laplacian_512").astype(dt)
+    x = synth.vector(0, m.cols).astype(dt)
+    y_ref = oracle_lib.csr_spmv(m.rows, m.row_ptr, m.columns, m.data, x)
+    assert np.array_equal(run(m, CSR_SCALAR, x), y_ref)  # rows of 5: default config is exact too
+    assert np.array_equal(run(m, ELL, x), y_ref)
+
+
+def _long_rows_matrix(dt):
+    rng = np.random.default_rng(77)
+    lens = rng.integers(0, 9, size=6000)
+    lens[[5, 1234, 5999]] = [50_000, 9_000, 4_097]
+    lens[[10, 11, 12]] = [3000, 0, 700]
+    cols = 200_000
+    rp = np.zeros(lens.size + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(cols, size=int(n), replace=False)) for n in lens]).astype(np.uint32)
+    v = rng.uniform(-1, 1, size=ci.size)
+    return F.csr_matrix_class.from_arrays(lens.size, cols, rp.astype(np.uint32), ci, v.astype(dt), dt)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("fmt", ALL)
+def test_long_rows_split_and_repeatable(oracle_lib, dt, fmt):
+    m = _long_rows_matrix(dt)
+    if fmt == ELL:
+        pytest.skip("ELL width 50,000")
+    x = synth.vector(3, m.cols).astype(dt)
+    ys = run(m, fmt, x, reps=3, hybrid_width=4)
+    check_tol(oracle_lib, m, x, ys[0], f"long rows fmt{fmt}")
+    # deterministic: counters and look-back state reset between launches
+    assert np.array_equal(ys[0], ys[1]) and np.array_equal(ys[1], ys[2])
+
+
+@pytest.mark.parametrize("lanes", [2, 4, 8, 16, 32])
+def test_vector_lane_counts(oracle_lib, lanes):
+    m = syn("power_law_300k").astype(np.float32)
+    x = synth.vector(1, m.cols).astype(np.float32)
+    check_tol(oracle_lib, m, x, run(m, CSR_VECTOR, x, {"vector_lanes": lanes}), f"lanes {lanes}")
+
+
+@pytest.mark.parametrize("cfg", [{"long_row_threshold": 300, "piece_nnz": 256}, {"assist_threshold": 8},
+                                 {"bin_nnz": 64}, {"bin_nnz": 700, "long_row_threshold": 5000}])
+@pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE])
+def test_csr_plan_configurations(oracle_lib, cfg, fmt):
+    m = _long_rows_matrix(np.float64)
+    x = synth.vector(5, m.cols)
+    check_tol(oracle_lib, m, x, run(m, fmt, x, cfg), f"cfg {cfg} fmt{fmt}")
+
+
+@pytest.mark.parametrize("fmt", ALL)
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_empty_rows_and_empty_matrix(fmt, dt):
+    rp = np.array([0, 0, 3, 3, 3, 4, 4], np.uint32)
+    ci = np.array([0, 2, 5, 1], np.uint32)
+    m = F.csr_matrix_class.from_arrays(6, 7, rp, ci, np.array([1, 2, 3, 4], dt), dt)
+    x = np.arange(1, 8).astype(dt)
+    y = run(m, fmt, x, hybrid_width=1)
+    assert np.array_equal(y, np.array([0, 1 + 6 + 18, 0, 0, 8, 0], dt))
+    z = F.csr_matrix_class.from_arrays(5, 3, np.zeros(6, np.uint32), np.zeros(0, np.uint32), np.zeros(0, dt), dt)
+    assert np.array_equal(run(z, fmt, np.ones(3, dt), hybrid_width=0), np.zeros(5, dt))
+
+
+def test_coo_tiles_sharing_rows(oracle_lib):
+    # one row spans many 2048-element tiles, separated by long runs of empty rows
+    rng = np.random.default_rng(5)
+    lens = np.zeros(100_000, np.int64)
+    lens[0] = 3
+    lens[17] = 20_000
+    lens[18] = 1
+    lens[60_000] = 9_000
+    lens[99_999] = 2
+    cols = 30_000
+    rp = np.zeros(lens.size + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(cols, size=int(n), replace=False)) for n in lens if n]).astype(np.uint32)
+    m = F.csr_matrix_class.from_arrays(lens.size, cols, rp.astype(np.uint32), ci, rng.uniform(-1, 1, ci.size), np.float64)
+    x = synth.vector(2, cols)
+    ys = run(m, COO, x, reps=3)
+    check_tol(oracle_lib, m, x, ys[0], "coo tiles")
+    assert np.array_equal(ys[0], ys[2])
+
+
+def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
+    m = syn("power_law_300k").astype(np.float32)
+    x = synth.vector(4, m.cols).astype(np.float32)
+    # offset every array by one element so the 16-byte paths are not taken
+    def dev(a):
+        t = torch.empty(a.size + 1, dtype=torch.from_numpy(a[:1]).dtype, device="cuda")
+        t[1:] = torch.from_numpy(a).cuda()
+        return t, t.data_ptr() + a.itemsize
+    _, d_v = dev(m.data)
+    _, d_c = dev(m.columns.view(np.int32))
+    _, d_r = dev(m.row_ptr.view(np.int32))
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.full((m.rows,), float("nan"), device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for algo in (0, 1, 2):
+        plan = C.c_void_p()
+        call("mfp_csr_plan_create", m.rows, m.cols, m.nnz, F.ptr(m.row_ptr), algo, None, C.byref(plan))
+        call("mfp_csr_spmv_f32", plan, C.c_void_p(d_v), C.c_void_p(d_c), C.c_void_p(d_r), C.c_void_p(xt.data_ptr()),
+             C.c_void_p(yt.data_ptr()), stream)
+        torch.cuda.synchronize()
+        check_tol(oracle_lib, m, x, yt.cpu().numpy(), f"unaligned csr algo {algo}")
+        call("mfp_csr_plan_destroy", plan)
+    coo = F.coo_matrix_class(m)
+    _, d_cv = dev(coo.data)
+    _, d_cc = dev(coo.cols_.view(np.int32))
+    _, d_cr = dev(coo.rows_.view(np.int32))
+    nbytes = C.c_size_t()
+    call("mfp_coo_workspace_bytes", m.rows, m.nnz, C.byref(nbytes))
+    ws = torch.zeros(nbytes.value, dtype=torch.uint8, device="cuda")
+    yt.fill_(float("nan"))
+    call("mfp_coo_spmv_f32", m.rows, m.cols, m.nnz, C.c_void_p(d_cv), C.c_void_p(d_cc), C.c_void_p(d_cr),
+         C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()), C.c_void_p(ws.data_ptr()), nbytes.value, stream)
+    torch.cuda.synchronize()
+    check_tol(oracle_lib, m, x, yt.cpu().numpy(), "unaligned coo")
+    err = C.c_uint32()
+    call("mfp_workspace_error", C.c_void_p(ws.data_ptr()), C.byref(err))
+    assert err.value == 0
+
+
+@pytest.mark.parametrize("fmt", [CSR_ADAPTIVE, COO, HYBRID])
+def test_host_buffer_call_equals_device_call(fmt):
+    m = syn("stencil_40").astype(np.float32)
+    x = synth.vector(8, m.cols).astype(np.float32)
+    dm = DeviceMatrix.build(m, fmt, hybrid_width=27)
+    y_host = np.empty(m.rows, np.float32)
+    dm.spmv_host(x, y_host)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty(m.rows, device="cuda")
+    dm.spmv(xt, yt)
+    torch.cuda.synchronize()
+    assert np.array_equal(y_host, yt.cpu().numpy())
+    info = dm.info()
+    assert info.nnz == m.nnz and info.algorithmic_bytes == m.nnz * 8 + (m.rows + 1) * 4 + m.cols * 4 + m.rows * 4
+
+
+@pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, COO, SCOO, HYBRID])
+def test_full_size_power_law_float32(oracle_lib, fmt):
+    """The power-law configuration at full size (4,194,304 rows, ~31M nnz)."""
+    if "power_law_full" not in SYN:
+        SYN["power_law_full"] = synth.power_law(seed=0).astype(np.float32)
+    m = SYN["power_law_full"]
+    x = synth.vector(0, m.cols).astype(np.float32)
+    hw = F.row_length_quantile(m, 2 / 3)
+    y = run(m, fmt, x, hybrid_width=hw)
+    check_tol(oracle_lib, m, x, y, f"power-law full fmt{fmt}")
+    # size-independent checksum: sum_i y_i = sum_j (column sum of A)_j x_j
+    colsum = np.bincount(m.columns, weights=m.data.astype(np.float64), minlength=m.cols)
+    assert abs(y.astype(np.float64).sum() - colsum @ x.astype(np.float64)) < 1e-3 * np.abs(m.data).sum() ** 0.5
