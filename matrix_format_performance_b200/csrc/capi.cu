@@ -321,7 +321,8 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
               const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const T *x, T *y,
               void *stream) {
   if (rows == 0) return ok();
-  if (!y || !sp || !v || !ci || !ri || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  // values / c_index / r_index may be NULL only when every slice is empty
+  if (!y || !sp || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   if (slice == 0 || (uint64_t)slice * slices < rows) return fail(MFP_ERROR_INVALID_VALUE, "slices do not cover the rows");
   const size_t acc_bytes = (size_t)((slice + 3u) & ~3u) * sizeof(T);
   if (win == nullptr) maxw = 0;
@@ -495,6 +496,12 @@ int finish_matrix(mfp_matrix *m, mfp_matrix **out) {
   return ok();
 }
 bool valid_vt(int vt) { return vt == MFP_F32 || vt == MFP_F64; }
+int check_columns(const uint32_t *c, uint64_t n, uint32_t cols) {
+  for (uint64_t i = 0; i < n; ++i)
+    if (c[i] >= cols && !(cols == 0 && c[i] == 0))
+      return fail(MFP_ERROR_INVALID_VALUE, "column id %u >= cols %u at %llu", c[i], cols, (unsigned long long)i);
+  return MFP_SUCCESS;
+}
 
 }  // namespace
 
@@ -516,6 +523,7 @@ int mfp_matrix_create_csr(int format, int vt, uint32_t rows, uint32_t cols, uint
   if (nnz && (!ci || !data)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
   int st = check_row_ptr(rows, nnz, rp);
   if (st) return st;
+  if ((st = check_columns(ci, nnz, cols))) return st;
   auto *m = new mfp_matrix();
   cudaGetDevice(&m->device);
   m->format = format;
@@ -542,6 +550,8 @@ int mfp_matrix_create_ell(int vt, uint32_t rows, uint32_t cols, uint32_t width, 
   if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
   const uint64_t slots = (uint64_t)rows * width;
   if (slots && (!ec || !ed)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  int st0 = check_columns(ec, slots, cols);
+  if (st0) return st0;
   const size_t vs = value_size(vt);
   auto *m = new mfp_matrix();
   cudaGetDevice(&m->device);
@@ -608,6 +618,21 @@ int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, c
   *out = nullptr;
   if (!valid_vt(vt) || !prm || !sp) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
   if (nnz && (!ci || !ri || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  {
+    int st0 = check_columns(ci, nnz, cols);
+    if (st0) return st0;
+    if ((uint64_t)prm->slice_size * prm->slices_count < rows)
+      return fail(MFP_ERROR_INVALID_VALUE, "slices do not cover the rows");
+    for (uint32_t s = 0; s < prm->slices_count; ++s) {
+      const uint32_t b = sp[s], e = sp[s + 1];
+      if (b >= e) continue;
+      if (e > nnz) return fail(MFP_ERROR_INVALID_VALUE, "slices_ptr[%u] beyond nnz", s + 1);
+      const uint64_t r0 = (uint64_t)s * prm->slice_size, r1 = std::min<uint64_t>(rows, r0 + prm->slice_size);
+      for (uint32_t k = b; k < e; ++k)
+        if (ri[k] < r0 || ri[k] >= r1 || (k > b && ri[k] < ri[k - 1]))
+          return fail(MFP_ERROR_INVALID_VALUE, "r_index[%u] outside slice %u or unsorted", k, s);
+    }
+  }
   const size_t vs = value_size(vt);
   auto *m = new mfp_matrix();
   cudaGetDevice(&m->device);
@@ -657,6 +682,10 @@ int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t widt
   for (uint32_t i = 0; i < cnnz; ++i) {
     if (cr[i] >= rows || cc[i] >= cols) return fail(MFP_ERROR_INVALID_VALUE, "tail index out of range at %u", i);
     if (i && cr[i] < cr[i - 1]) return fail(MFP_ERROR_INVALID_VALUE, "tail rows must be sorted (element %u)", i);
+  }
+  {
+    int st0 = check_columns(ec, slots, cols);
+    if (st0) return st0;
   }
   const size_t vs = value_size(vt);
   auto *m = new mfp_matrix();

@@ -74,8 +74,8 @@ int csr_from_coo(uint32_t rows, uint32_t cols, uint32_t nnz, int scheme, const u
 template <typename T>
 int ell_from_csr(uint32_t rows, const uint32_t *rp, const uint32_t *columns, const T *data,
                  uint32_t width, T *ed, uint32_t *ec) {
-  if (!rp || !ed || !ec) return fail(MFP_ERROR_INVALID_VALUE, "null array");
   const size_t n = (size_t)rows * width;
+  if (!rp || (n && (!ed || !ec))) return fail(MFP_ERROR_INVALID_VALUE, "null array");
   std::fill_n(ed, n, T(0));
   std::fill_n(ec, n, 0u);
   for (uint32_t r = 0; r < rows; ++r) {

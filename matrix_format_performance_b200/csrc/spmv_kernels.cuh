@@ -681,6 +681,19 @@ __global__ void __launch_bounds__(kBlock) coo_kernel(uint32_t n_rows, uint32_t n
   if (threadIdx.x == 0) sm.tile = atomicAdd(&ws->ticket, 1u);
   __syncthreads();
   const uint32_t tile = sm.tile;
+  if (tile >= gridDim.x) {
+    // the workspace was not left zeroed (an interrupted launch): refuse the
+    // tile instead of reading past the arrays; the host sees the error word
+    if (threadIdx.x == 0) {
+      atomicOr(&ws->error, 2u);
+      const uint32_t d = atomicAdd(&ws->done, 1u);
+      if (d == gridDim.x - 1) {
+        ws->ticket = 0u;
+        ws->done = 0u;
+      }
+    }
+    return;
+  }
   const uint32_t c0 = tile * (uint32_t)kChunk;
   const uint32_t c1 = min(nnz, c0 + (uint32_t)kChunk);
   const uint32_t p = c0 > 0 ? rows[c0 - 1] : kNoRow;
@@ -744,8 +757,8 @@ __global__ void __launch_bounds__(kBlock) coo_kernel(uint32_t n_rows, uint32_t n
           ok = false;
           break;
         }
-        const T v = tiles[c].value;
-        const uint32_t kind = tiles[c].kind;
+        const T v = __ldcg(&tiles[c].value);
+        const uint32_t kind = __ldcg(&tiles[c].kind);
         tiles[c].flag = 0u;  // consumed
         sum = add_rn(v, sum);
         if (kind != 2u) break;

@@ -224,6 +224,6 @@ def compare_results(a: np.ndarray, b: np.ndarray) -> tuple[float, int | None]:
     assert a.dtype == b.dtype and a.size == b.size
     err = C.c_double()
     bad = C.c_uint32()
-    call(f"mfp_compare_results_{_SFX[a.dtype]}", a.size, ptr(np.ascontiguousarray(a)),
-         ptr(np.ascontiguousarray(b)), C.byref(err), C.byref(bad))
+    aa, bb = np.ascontiguousarray(a), np.ascontiguousarray(b)  # alive across the call
+    call(f"mfp_compare_results_{_SFX[a.dtype]}", a.size, ptr(aa), ptr(bb), C.byref(err), C.byref(bad))
     return err.value, (None if bad.value == 0xFFFFFFFF else int(bad.value))

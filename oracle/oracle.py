@@ -78,28 +78,31 @@ class Oracle:
     # -- SpMV ---------------------------------------------------------------
     def csr_spmv(self, rows, row_ptr, cols, data, x, reduce_order=False) -> np.ndarray:
         y = np.empty(rows, data.dtype)
+        xx = np.ascontiguousarray(x, data.dtype)  # keep alive across the call
         fn = f"oracle_csr_spmv{'_reduce_order' if reduce_order else ''}_{self._sfx(data.dtype)}"
-        getattr(self.lib, fn)(rows, _p(row_ptr), _p(cols), _p(data), _p(np.ascontiguousarray(x, data.dtype)), _p(y))
+        getattr(self.lib, fn)(rows, _p(row_ptr), _p(cols), _p(data), _p(xx), _p(y))
         return y
 
     def ell_spmv(self, rows, width, data, cols, x) -> np.ndarray:
         y = np.empty(rows, data.dtype)
-        getattr(self.lib, f"oracle_ell_spmv_{self._sfx(data.dtype)}")(rows, width, _p(data), _p(cols),
-                                                                      _p(np.ascontiguousarray(x, data.dtype)), _p(y))
+        xx = np.ascontiguousarray(x, data.dtype)
+        getattr(self.lib, f"oracle_ell_spmv_{self._sfx(data.dtype)}")(rows, width, _p(data), _p(cols), _p(xx), _p(y))
         return y
 
     def csr_spmv_exact(self, rows, row_ptr, cols, data, x) -> tuple[np.ndarray, np.ndarray]:
         """(y, sum |a x|) in extended precision; data/x are converted to float64 exactly."""
         y = np.empty(rows, np.float64)
         ab = np.empty(rows, np.float64)
-        self.lib.oracle_csr_spmv_ld(rows, _p(row_ptr), _p(cols), _p(np.ascontiguousarray(data, np.float64)),
-                                    _p(np.ascontiguousarray(x, np.float64)), _p(y), _p(ab))
+        dd = np.ascontiguousarray(data, np.float64)
+        xx = np.ascontiguousarray(x, np.float64)
+        self.lib.oracle_csr_spmv_ld(rows, _p(row_ptr), _p(cols), _p(dd), _p(xx), _p(y), _p(ab))
         return y, ab
 
     def csr_spmv_parallel(self, threads, rows, row_ptr, cols, data, x) -> tuple[np.ndarray, float]:
         y = np.empty(rows, data.dtype)
+        xx = np.ascontiguousarray(x, data.dtype)
         t = self.lib.oracle_csr_spmv_parallel(threads, int(data.dtype == np.float64), rows, _p(row_ptr), _p(cols),
-                                              _p(data), _p(np.ascontiguousarray(x, data.dtype)), _p(y))
+                                              _p(data), _p(xx), _p(y))
         return y, t
 
     # -- converters ---------------------------------------------------------

@@ -216,9 +216,15 @@ def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
         t = torch.empty(a.size + 1, dtype=torch.from_numpy(a[:1]).dtype, device="cuda")
         t[1:] = torch.from_numpy(a).cuda()
         return t, t.data_ptr() + a.itemsize
-    _, d_v = dev(m.data)
-    _, d_c = dev(m.columns.view(np.int32))
-    _, d_r = dev(m.row_ptr.view(np.int32))
+    keep = []  # the tensors must outlive the raw pointers handed to the library
+
+    def dev_keep(a):
+        t, p = dev(a)
+        keep.append(t)
+        return p
+    d_v = dev_keep(m.data)
+    d_c = dev_keep(m.columns.view(np.int32))
+    d_r = dev_keep(m.row_ptr.view(np.int32))
     xt = torch.from_numpy(x).cuda()
     yt = torch.full((m.rows,), float("nan"), device="cuda")
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -231,9 +237,9 @@ def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
         check_tol(oracle_lib, m, x, yt.cpu().numpy(), f"unaligned csr algo {algo}")
         call("mfp_csr_plan_destroy", plan)
     coo = F.coo_matrix_class(m)
-    _, d_cv = dev(coo.data)
-    _, d_cc = dev(coo.cols_.view(np.int32))
-    _, d_cr = dev(coo.rows_.view(np.int32))
+    d_cv = dev_keep(coo.data)
+    d_cc = dev_keep(coo.cols_.view(np.int32))
+    d_cr = dev_keep(coo.rows_.view(np.int32))
     nbytes = C.c_size_t()
     call("mfp_coo_workspace_bytes", m.rows, m.nnz, C.byref(nbytes))
     ws = torch.zeros(nbytes.value, dtype=torch.uint8, device="cuda")
