@@ -202,8 +202,7 @@ def run_engine(args):
     import torch.distributed as dist
 
     from matrix_format_performance_b200 import formats as F
-    from matrix_format_performance_b200.device import (COO, CSR_ADAPTIVE, CSR_SCALAR, CSR_VECTOR, HYBRID, LABELS,
-                                                       SCOO, DeviceMatrix, device_info)
+    from matrix_format_performance_b200.device import LABELS, DeviceMatrix, device_info
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -213,12 +212,14 @@ def run_engine(args):
     dev = device_info(local)
     m, x = build_workload(args.rows, seed=rank)
     hyb_w = F.row_length_quantile(m, 2 / 3)
-    formats = [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, COO, SCOO, HYBRID]
+    from matrix_format_performance_b200.device import FORMAT_NAMES
+    formats = [FORMAT_NAMES[n] for n in args.formats.split(",")]
     mats = {}
     t = time.time()
     for f in formats:
+        cfg = {"kernel": args.csr_kernel} if f in (0, 1, 2) and args.csr_kernel else None
         mats[f] = DeviceMatrix.build(m, f, sm_count=dev.sm_count, shared_mem=int(dev.shared_mem_per_block),
-                                     hybrid_width=hyb_w)
+                                     hybrid_width=hyb_w, config=cfg)
     log(f"[bench] rank {rank}: formats uploaded in {time.time() - t:.1f}s (hybrid ELL width {hyb_w})")
     skipped = {"GPU ELL": f"padding: width {int(m.row_lengths().max())} x {m.rows} rows "
                           f"= {int(m.row_lengths().max()) * m.rows * 8 / 1e12:.2f} TB"}
@@ -325,8 +326,7 @@ def run_engine(args):
                "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
                        "h2d_bytes_per_step": int(m.cols * 4 * len(formats) * ws),
                        "d2h_bytes_per_step": int(m.rows * 4 * len(formats) * ws), "steps": e_steps},
-               "gpu_launches": args.steps * len(formats) * sum(
-                   mats[f].info().kernel_launches for f in formats) // len(formats),
+               "gpu_launches": args.steps * sum(mats[f].info().kernel_launches for f in formats),
                "clocks": clocks}
         if ws == 1 and not args.no_cpu_baseline:
             try:
@@ -351,6 +351,10 @@ def main():
     ap.add_argument("--rows", type=int, default=4_194_304)
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--csr-kernel", type=int, default=0,
+                    help="CSR kernel: 0 auto, 1 row-block, 2 streaming (2048-element chunks), 3 streaming (1024)")
+    ap.add_argument("--formats", default="csr,csr_vector,csr_adaptive,coo,scoo,hybrid",
+                    help="comma list of: csr, csr_vector, csr_adaptive, coo, scoo, hybrid")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "engine":
         log("[bench] warm-up raised to 3 (the timing rules require at least 3)")

@@ -166,6 +166,9 @@ typedef struct mfp_csr_config {
   uint32_t assist_threshold;   /* scalar/vector: rows longer than this (and not long) are
                                   reduced by a whole warp; 0 = default (64);
                                   UINT32_MAX = never (keeps the reference summation order) */
+  uint32_t kernel;             /* 0 = auto, 1 = row-block kernel (rows per CTA, long rows in
+                                  pieces), 2 = streaming kernel (fixed element chunks per
+                                  persistent CTA, TMA bulk prefetch) */
 } mfp_csr_config;
 typedef struct mfp_csr_plan mfp_csr_plan;
 int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *host_row_ptr,

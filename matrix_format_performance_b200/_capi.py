@@ -10,7 +10,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libmfp_spmv.so"
+# MFP_LIBRARY selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = Path(os.environ.get("MFP_LIBRARY", Path(__file__).resolve().parent / "lib" / "libmfp_spmv.so"))
 
 u32, u64, i32, f64 = C.c_uint32, C.c_uint64, C.c_int, C.c_double
 vp = C.c_void_p
@@ -34,7 +35,7 @@ class ScooParams(C.Structure):
 
 class CsrConfig(C.Structure):
     _fields_ = [("long_row_threshold", u32), ("vector_lanes", u32), ("bin_nnz", u32),
-                ("piece_nnz", u32), ("assist_threshold", u32)]
+                ("piece_nnz", u32), ("assist_threshold", u32), ("kernel", u32)]
 
 
 class MatrixInfo(C.Structure):

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["capi.cu"]
 CPP_SOURCES = ["util.cpp", "formats.cpp", "synth.cpp"]
-HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "host_common.h"]
+HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "spmv_stream.cuh", "host_common.h"]
 
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3",
                      "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]
@@ -51,35 +51,40 @@ def _run(cmd: list[str]) -> None:
         sys.stderr.write(r.stderr)
 
 
-def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
-    LIBDIR.mkdir(exist_ok=True)
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False, defines: list[str] | None = None,
+          out: Path | None = None, objdir: Path | None = None) -> Path:
+    """Compiles and links the library; `defines` (e.g. ["MFP_CSR_MINBLOCKS=6"]) build a variant into `out`."""
+    build_dir = objdir or BUILD
+    lib = out or LIB
+    build_dir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(parents=True, exist_ok=True)
+    dflags = [f"-D{d}" for d in (defines or [])]
     headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "mfp_spmv.h"]
     tasks = []
     objs = []
     for src in CU_SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = build_dir / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            tasks.append([NVCC] + NVCC_FLAGS + ["-c", str(s), "-o", str(o)])
+            tasks.append([NVCC] + NVCC_FLAGS + dflags + ["-c", str(s), "-o", str(o)])
     for src in CPP_SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = build_dir / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            tasks.append(["g++"] + CXX_FLAGS + ["-c", str(s), "-o", str(o)])
+            tasks.append(["g++"] + CXX_FLAGS + dflags + ["-c", str(s), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
         for f in [ex.submit(_run, t) for t in tasks]:
             f.result()
-    if force or tasks or _stale(LIB, objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if force or tasks or _stale(lib, objs):
+        tmp = lib.with_suffix(".so.tmp")
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
              + ["-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib)
     if verbose:
-        print(f"built {LIB}")
-    return LIB
+        print(f"built {lib}")
+    return lib
 
 
 def clean() -> None:

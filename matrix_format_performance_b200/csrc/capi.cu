@@ -1,6 +1,7 @@
 // C ABI: plans, kernel launches, device-resident matrix handles and timing.
 #include "host_common.h"
 #include "spmv_kernels.cuh"
+#include "spmv_stream.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -57,7 +58,47 @@ int upload(T **p, const T *host, size_t count, size_t *acct = nullptr) {
 // ---------------------------------------------------------------------------
 // CSR plan
 // ---------------------------------------------------------------------------
+namespace {
+// Streaming CSR kernel variants: chunk of CH elements, S pipeline stages.
+// Variant 0 (config.kernel = 2): 2048-element chunks; variant 1 (= 3):
+// 1024-element chunks with a deeper ring.
+template <typename T, int V>
+struct stream_cfg;
+template <>
+struct stream_cfg<float, 0> {
+  static constexpr int CH = 2048, S = 3;
+};
+template <>
+struct stream_cfg<double, 0> {
+  static constexpr int CH = 2048, S = 2;
+};
+template <>
+struct stream_cfg<float, 1> {
+  static constexpr int CH = 1024, S = 4;
+};
+template <>
+struct stream_cfg<double, 1> {
+  static constexpr int CH = 1024, S = 3;
+};
+template <typename T, int V>
+constexpr size_t stream_smem_bytes() {
+  using C = stream_cfg<T, V>;
+  return sizeof(d::stream_smem<T, C::CH, C::S>) + d::kCrowCap * sizeof(uint32_t);
+}
+struct stream_plan {
+  uint32_t chunk = 0, nchunks = 0;
+  uint32_t *chunk_row = nullptr;
+  uint32_t grid = 0, chunks_per_cta = 0, n_contrib = 0, slots = 0;
+  d::stream_edge *edges = nullptr;
+  d::long_piece *contrib = nullptr;
+  double *partials = nullptr;
+  uint32_t *counters = nullptr;
+};
+}  // namespace
+
 struct mfp_csr_plan {
+  uint32_t *error = nullptr;
+  stream_plan sp[2];  // per value type (f32, f64): chunking and grid depend on both
   int device = 0;
   int algo = 0;
   mfp_csr_config cfg{};
@@ -78,6 +119,112 @@ constexpr uint32_t kDefaultPiece = 4096;
 constexpr uint32_t kFp64Rows = 4096;  // rows longer than this accumulate in FP64
 constexpr uint32_t kMaxBin = d::kChunk - 4;
 }  // namespace
+
+namespace {
+template <typename T, int V, int MODE>
+int stream_occupancy() {
+  using C = stream_cfg<T, V>;
+  auto k = d::csr_stream_kernel<T, MODE, C::CH, C::S>;
+  const int smem = (int)stream_smem_bytes<T, V>();
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) cudaGetLastError();
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, d::kBlock, smem) != cudaSuccess) {
+    cudaGetLastError();
+    blocks = 2;
+  }
+  return std::max(1, blocks);
+}
+template <typename T, int V>
+int stream_occupancy_algo(int algo) {
+  return algo == 0 ? stream_occupancy<T, V, 0>() : algo == 1 ? stream_occupancy<T, V, 1>() : stream_occupancy<T, V, 2>();
+}
+
+// Fixed chunks of `chunk` elements, statically partitioned over `target`
+// persistent CTAs, and the contributions of the rows split between two CTA
+// ranges (an ordered partial-sum slot per CTA the row touches).
+int build_stream_plan(stream_plan &sp, uint32_t rows, uint32_t nnz, const uint32_t *rp, uint32_t chunk,
+                      uint32_t target, size_t *acct) {
+  sp.chunk = chunk;
+  sp.nchunks = ceil_div(nnz, chunk);
+  if (sp.nchunks == 0) return MFP_SUCCESS;
+  std::vector<uint32_t> cr((size_t)sp.nchunks + 1);
+  for (uint32_t k = 0; k < sp.nchunks; ++k)
+    cr[k] = (uint32_t)(std::lower_bound(rp, rp + rows + 1, k * chunk) - rp);
+  cr[sp.nchunks] = rows;
+  const uint32_t K = ceil_div(sp.nchunks, std::max(1u, target));
+  sp.chunks_per_cta = K;
+  sp.grid = ceil_div(sp.nchunks, K);
+  const uint64_t span = (uint64_t)K * chunk;  // elements per CTA
+  std::vector<d::stream_edge> edges(sp.grid, d::stream_edge{d::kNoPiece, d::kNoPiece});
+  std::vector<d::long_piece> contrib;
+  uint32_t slots = 0, counter = 0;
+  uint32_t last_row = UINT32_MAX;
+  for (uint32_t c = 0; c + 1 < sp.grid; ++c) {
+    const uint64_t C1 = std::min<uint64_t>((uint64_t)(c + 1) * span, nnz);
+    // the row holding element C1 - 1, if it continues past C1
+    const uint32_t r = (uint32_t)(std::upper_bound(rp, rp + rows + 1, (uint32_t)(C1 - 1)) - rp) - 1;
+    if (rp[r + 1] <= C1 || r == last_row) continue;
+    last_row = r;
+    const uint32_t cs = (uint32_t)(rp[r] / span), ce = (uint32_t)((rp[r + 1] - 1) / span);
+    const uint32_t np = ce - cs + 1;
+    for (uint32_t q = cs; q <= ce; ++q) {
+      d::long_piece pc{};
+      pc.row = r;
+      pc.slot_base = slots;
+      pc.piece = q - cs;
+      pc.npieces = np;
+      pc.counter = counter;
+      pc.fp64 = (rp[r + 1] - rp[r]) > kFp64Rows;
+      const uint32_t idx = (uint32_t)contrib.size();
+      contrib.push_back(pc);
+      if (q != cs) edges[q].head = idx;
+      if (q != ce) edges[q].tail = idx;
+    }
+    slots += np;
+    ++counter;
+  }
+  sp.n_contrib = (uint32_t)contrib.size();
+  sp.slots = slots;
+  int st;
+  if ((st = upload(&sp.chunk_row, cr.data(), cr.size(), acct)) ||
+      (st = upload(&sp.edges, edges.data(), edges.size(), acct)) ||
+      (st = upload(&sp.contrib, contrib.data(), contrib.size(), acct)) ||
+      (st = dmalloc(&sp.partials, slots, acct)) || (st = dmalloc(&sp.counters, counter, acct)))
+    return st;
+  if (counter) CUDA_TRY(cudaMemset(sp.counters, 0, counter * sizeof(uint32_t)), "cudaMemset counters");
+  return MFP_SUCCESS;
+}
+
+void free_stream_plan(stream_plan &sp) {
+  cudaFree(sp.chunk_row);
+  cudaFree(sp.edges);
+  cudaFree(sp.contrib);
+  cudaFree(sp.partials);
+  cudaFree(sp.counters);
+  sp = stream_plan{};
+}
+}  // namespace
+
+// Streaming-kernel plans for both value types; variant from config.kernel.
+int build_stream_plans(mfp_csr_plan *plan, const uint32_t *rp) {
+  if (plan->nnz == 0 || plan->cfg.kernel < 2) return MFP_SUCCESS;
+  int st;
+  if ((st = dmalloc(&plan->error, 1, &plan->device_bytes))) return st;
+  CUDA_TRY(cudaMemset(plan->error, 0, sizeof(uint32_t)), "cudaMemset error word");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device);
+  const bool v1 = plan->cfg.kernel == 3;
+  const int occ32 = v1 ? stream_occupancy_algo<float, 1>(plan->algo) : stream_occupancy_algo<float, 0>(plan->algo);
+  const int occ64 = v1 ? stream_occupancy_algo<double, 1>(plan->algo) : stream_occupancy_algo<double, 0>(plan->algo);
+  const uint32_t ch32 = v1 ? stream_cfg<float, 1>::CH : stream_cfg<float, 0>::CH;
+  const uint32_t ch64 = v1 ? stream_cfg<double, 1>::CH : stream_cfg<double, 0>::CH;
+  if ((st = build_stream_plan(plan->sp[0], plan->rows, plan->nnz, rp, ch32, (uint32_t)(sms * occ32),
+                              &plan->device_bytes)) ||
+      (st = build_stream_plan(plan->sp[1], plan->rows, plan->nnz, rp, ch64, (uint32_t)(sms * occ64),
+                              &plan->device_bytes)))
+    return st;
+  return MFP_SUCCESS;
+}
 
 extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
                                    int algo, const mfp_csr_config *config, mfp_csr_plan **out) {
@@ -167,6 +314,10 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
   }
   plan->n_pieces = (uint32_t)pieces.size();
   plan->n_long = nlong;
+  if ((st = build_stream_plans(plan, rp))) {
+    mfp_csr_plan_destroy(plan);
+    return st;
+  }
   if ((uint64_t)plan->n_main + plan->n_pieces > 0x7fffffffull) {
     delete plan;
     return fail(MFP_ERROR_TOO_LARGE, "grid too large");
@@ -195,6 +346,9 @@ extern "C" int mfp_csr_plan_destroy(mfp_csr_plan *plan) {
   cudaFree(plan->partials);
   cudaFree(plan->counters);
   cudaFree(plan->row_blocks);
+  cudaFree(plan->error);
+  free_stream_plan(plan->sp[0]);
+  free_stream_plan(plan->sp[1]);
   delete plan;
   return ok();
 }
@@ -214,6 +368,20 @@ extern "C" int mfp_csr_plan_get_config(const mfp_csr_plan *plan, int *algo, mfp_
 
 namespace {
 template <typename T>
+int fill(uint64_t n, T *v, T value, void *stream);
+
+template <typename T, int V>
+void launch_stream(int algo, uint32_t grid, cudaStream_t s, const d::stream_args<T> &S) {
+  using C = stream_cfg<T, V>;
+  const size_t smem = stream_smem_bytes<T, V>();
+  switch (algo) {
+    case 0: d::csr_stream_kernel<T, 0, C::CH, C::S><<<grid, d::kBlock, smem, s>>>(S); break;
+    case 1: d::csr_stream_kernel<T, 1, C::CH, C::S><<<grid, d::kBlock, smem, s>>>(S); break;
+    default: d::csr_stream_kernel<T, 2, C::CH, C::S><<<grid, d::kBlock, smem, s>>>(S); break;
+  }
+}
+
+template <typename T>
 int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, const uint32_t *rp, const T *x,
              T *y, void *stream) {
   if (!plan) return fail(MFP_ERROR_INVALID_VALUE, "plan is NULL");
@@ -231,13 +399,45 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
   A.lanes = plan->cfg.vector_lanes ? plan->cfg.vector_lanes : 32;
   A.row_blocks = plan->row_blocks;
   A.n_main = plan->n_main;
+  A.n_pieces = plan->n_pieces;
   A.pieces = plan->pieces;
   A.partials = plan->partials;
   A.counters = plan->counters;
   const bool vec = aligned16(data) && aligned16(cols);
+  cudaStream_t s = as_stream(stream);
+  if (plan->nnz == 0) return fill<T>(plan->rows, y, T(0), stream);
+  const stream_plan &sp = plan->sp[sizeof(T) == 8 ? 1 : 0];
+  // the exact-order configuration keeps every row in one thread's sequential
+  // sum, which only the row-block kernel does for rows split between CTAs
+  const bool exact_order = plan->cfg.long_row_threshold == UINT32_MAX && plan->assist_thr == UINT32_MAX;
+  if (vec && aligned16(rp) && sp.grid && !exact_order && plan->cfg.kernel >= 2) {
+    d::stream_args<T> S{};
+    S.n_rows = plan->rows;
+    S.nnz = plan->nnz;
+    S.nchunks = sp.nchunks;
+    S.chunks_per_cta = sp.chunks_per_cta;
+    S.row_ptr = rp;
+    S.cols = cols;
+    S.vals = data;
+    S.x = x;
+    S.y = y;
+    S.chunk_row = sp.chunk_row;
+    S.edges = sp.edges;
+    S.contrib = sp.contrib;
+    S.partials = sp.partials;
+    S.counters = sp.counters;
+    S.error = plan->error;
+    S.assist_thr = plan->assist_thr;
+    S.lanes = A.lanes;
+    S.fp64_thr = kFp64Rows;
+    if (plan->cfg.kernel == 3)
+      launch_stream<T, 1>(plan->algo, sp.grid, s, S);
+    else
+      launch_stream<T, 0>(plan->algo, sp.grid, s, S);
+    return check_launch("csr_stream_kernel launch");
+  }
   const uint32_t grid = plan->n_main + plan->n_pieces;
   if (grid == 0) return ok();
-  cudaStream_t s = as_stream(stream);
 #define MFP_CSR_LAUNCH(ALGO)                                                         \
   if (vec)                                                                           \
     d::csr_kernel<T, ALGO, true><<<grid, d::kBlock, 0, s>>>(A);                      \
@@ -307,13 +507,26 @@ int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32
                 const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
                 const T *x, T *y) {
   auto k = d::scoo_kernel<T, VEC, XWIN>;
-  static std::once_flag once;
-  std::call_once(once, [&] {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         227 * 1024 - (int)sizeof(d::scoo_smem_static<T>));
-  });
+  // raise the kernel's dynamic shared-memory limit when a launch needs more
+  static std::mutex mu;
+  static size_t limit = 0;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (dyn > limit && dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MFP_ERROR_CUDA, "cudaFuncSetAttribute(scoo_kernel, %zu dynamic bytes, %zu static): %s", dyn,
+                    sizeof(d::scoo_smem_static<T>), cudaGetErrorString(e));
+      }
+      limit = dyn;
+    }
+  }
   k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, x, y);
-  return check_launch("scoo_kernel launch");
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(MFP_ERROR_CUDA, "scoo_kernel launch (grid %u, %zu dynamic bytes): %s", grid, dyn, cudaGetErrorString(e));
+  return ok();
 }
 
 template <typename T>

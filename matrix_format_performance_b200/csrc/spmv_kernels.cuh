@@ -31,6 +31,16 @@
 namespace mfp {
 namespace dev {
 
+// Tuning knobs (compile-time): CTAs per SM the CSR kernel is register-limited
+// to, and whether long-row pieces take the first block indices.  Measured on
+// the power-law configuration: 8 CTAs per SM and pieces last are fastest.
+#ifndef MFP_CSR_MINBLOCKS
+#define MFP_CSR_MINBLOCKS 8
+#endif
+#ifndef MFP_PIECES_FIRST
+#define MFP_PIECES_FIRST 0
+#endif
+
 constexpr int kBlock = 256;   // threads per CTA for every kernel
 constexpr int kEpt = 8;       // staged elements per thread
 constexpr int kChunk = kBlock * kEpt;  // elements staged per phase
@@ -287,6 +297,40 @@ __device__ __forceinline__ void block_segmented_reduce(const T *s_prod, const ui
   }
 }
 
+// acc + p[lo] + p[lo+1] + ... + p[hi-1] in that order (exact CSR order);
+// UNROLL keeps four shared-memory loads in flight per step (faster for long
+// segments, costs registers).
+template <typename T, bool UNROLL = true>
+__device__ __forceinline__ T seq_sum(T acc, const T *prod, uint32_t lo, uint32_t hi) {
+  uint32_t i = lo;
+  for (; UNROLL && i + 4 <= hi; i += 4) {
+    const T a = prod[swz(i)], b = prod[swz(i + 1)], c = prod[swz(i + 2)], d = prod[swz(i + 3)];
+    acc = add_rn(acc, a);
+    acc = add_rn(acc, b);
+    acc = add_rn(acc, c);
+    acc = add_rn(acc, d);
+  }
+  for (; i < hi; ++i) acc = add_rn(acc, prod[swz(i)]);
+  return acc;
+}
+
+// Lane-strided partial sum over [lo, hi) with stride L starting at lo + lane,
+// four loads in flight per step (same order as the one-at-a-time loop).
+template <typename T, bool UNROLL = true>
+__device__ __forceinline__ T strided_sum(const T *prod, uint32_t lo, uint32_t hi, uint32_t lane, uint32_t L) {
+  T acc = T(0);
+  uint32_t i = lo + lane;
+  for (; UNROLL && i + 3 * L < hi; i += 4 * L) {
+    const T a = prod[swz(i)], b = prod[swz(i + L)], c = prod[swz(i + 2 * L)], d = prod[swz(i + 3 * L)];
+    acc = add_rn(acc, a);
+    acc = add_rn(acc, b);
+    acc = add_rn(acc, c);
+    acc = add_rn(acc, d);
+  }
+  for (; i < hi; i += L) acc = add_rn(acc, prod[swz(i)]);
+  return acc;
+}
+
 // ---------------------------------------------------------------------------
 // Long-row pieces (CSR family)
 // ---------------------------------------------------------------------------
@@ -300,74 +344,101 @@ struct long_piece {
   uint32_t fp64;       // 1: accumulate in FP64 (rows longer than 4096)
 };
 
+// Whole-CTA dot product of vals[e] * x[cols[e]] over e in [a, b).  Each
+// thread takes 8 elements per round (two 4-element groups) and issues all of
+// a round's streaming loads before its first x gather, so a round costs one
+// DRAM and one L2 round trip.  Acc is T (plain) or comp_sum (FP64).
+template <typename T, bool VEC>
+struct acc_plain {
+  T v = T(0);
+  __device__ __forceinline__ void add(T p) { v = add_rn(v, p); }
+  __device__ __forceinline__ void add_prod(T a, T xv) { v = add_rn(v, mul_rn(a, xv)); }
+};
+template <typename T, bool VEC>
+struct acc_fp64 {
+  comp_sum v;
+  __device__ __forceinline__ void add_prod(T a, T xv) { v.add(__dmul_rn((double)a, (double)xv)); }
+};
+
+template <typename T, bool VEC, typename ACC>
+__device__ __forceinline__ void cta_range_dot(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                              const T *__restrict__ x, uint32_t a, uint32_t b, ACC &acc,
+                                              uint64_t pol) {
+  uint32_t s0 = a, s1 = b;
+  if (VEC) {
+    const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
+    if (a4 < b4) {
+      const uint32_t ng = (b4 - a4) >> 2;
+      uint32_t g = threadIdx.x;
+      for (; g + kBlock < ng; g += 2 * kBlock) {
+        T v[2][4];
+        uint32_t c[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          ld_stream4(vals + a4 + 4u * (g + u * kBlock), v[u], pol);
+          ld_stream4(cols + a4 + 4u * (g + u * kBlock), c[u], pol);
+        }
+        T xv[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) xv[u][k] = ld_x(x + c[u][k]);
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc.add_prod(v[u][k], xv[u][k]);
+      }
+      for (; g < ng; g += kBlock) {
+        T v[4];
+        uint32_t c[4];
+        ld_stream4(vals + a4 + 4u * g, v, pol);
+        ld_stream4(cols + a4 + 4u * g, c, pol);
+        T xv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) xv[k] = ld_x(x + c[k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc.add_prod(v[k], xv[k]);
+      }
+      if (threadIdx.x < a4 - a) {
+        const uint32_t e = a + threadIdx.x;
+        acc.add_prod(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+      }
+      if (threadIdx.x < b - b4) {
+        const uint32_t e = b4 + threadIdx.x;
+        acc.add_prod(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+      }
+      return;
+    }
+  }
+  uint32_t e = s0 + threadIdx.x;
+  for (; e + 3 * kBlock < s1; e += 4 * kBlock) {
+    T v[4];
+    uint32_t c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      v[u] = ld_stream1(vals + e + u * kBlock, pol);
+      c[u] = ld_stream1(cols + e + u * kBlock, pol);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc.add_prod(v[u], ld_x(x + c[u]));
+  }
+  for (; e < s1; e += kBlock) acc.add_prod(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
+}
+
 template <typename T, bool VEC>
 __device__ __forceinline__ void run_piece(const long_piece &pc, const T *__restrict__ vals,
                                           const uint32_t *__restrict__ cols, const T *__restrict__ x,
                                           T *__restrict__ y, double *partials, uint32_t *counters,
                                           double *s_a, double *s_b, uint64_t pol) {
-  const uint32_t a = pc.e0, b = pc.e1;
   double result;
   if (pc.fp64) {
-    comp_sum acc;
-    uint32_t s0 = a, s1 = b;
-    if (VEC) {
-      const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
-      if (a4 < b4) {
-        const uint32_t ng = (b4 - a4) >> 2;
-        for (uint32_t g = threadIdx.x; g < ng; g += kBlock) {
-          const uint32_t e0 = a4 + 4u * g;
-          T v[4];
-          uint32_t c[4];
-          ld_stream4(vals + e0, v, pol);
-          ld_stream4(cols + e0, c, pol);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) acc.add(__dmul_rn((double)v[k], (double)ld_x(x + c[k])));
-        }
-        if (threadIdx.x < a4 - a) {
-          const uint32_t e = a + threadIdx.x;
-          acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
-        }
-        if (threadIdx.x < b - b4) {
-          const uint32_t e = b4 + threadIdx.x;
-          acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
-        }
-        s0 = s1 = 0;
-      }
-    }
-    for (uint32_t e = s0 + threadIdx.x; e < s1; e += kBlock)
-      acc.add(__dmul_rn((double)ld_stream1(vals + e, pol), (double)ld_x(x + ld_stream1(cols + e, pol))));
-    const comp_sum r = block_reduce_comp<kBlock>(acc, s_a, s_b);
-    result = r.value();
+    acc_fp64<T, VEC> acc;
+    cta_range_dot<T, VEC>(vals, cols, x, pc.e0, pc.e1, acc, pol);
+    result = block_reduce_comp<kBlock>(acc.v, s_a, s_b).value();
   } else {
-    T acc = T(0);
-    uint32_t s0 = a, s1 = b;
-    if (VEC) {
-      const uint32_t a4 = (a + 3u) & ~3u, b4 = b & ~3u;
-      if (a4 < b4) {
-        const uint32_t ng = (b4 - a4) >> 2;
-        for (uint32_t g = threadIdx.x; g < ng; g += kBlock) {
-          const uint32_t e0 = a4 + 4u * g;
-          T v[4];
-          uint32_t c[4];
-          ld_stream4(vals + e0, v, pol);
-          ld_stream4(cols + e0, c, pol);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) acc = add_rn(acc, mul_rn(v[k], ld_x(x + c[k])));
-        }
-        if (threadIdx.x < a4 - a) {
-          const uint32_t e = a + threadIdx.x;
-          acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
-        }
-        if (threadIdx.x < b - b4) {
-          const uint32_t e = b4 + threadIdx.x;
-          acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
-        }
-        s0 = s1 = 0;
-      }
-    }
-    for (uint32_t e = s0 + threadIdx.x; e < s1; e += kBlock)
-      acc = add_rn(acc, mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol))));
-    result = (double)block_reduce<T, kBlock>(acc, reinterpret_cast<T *>(s_a));
+    acc_plain<T, VEC> acc;
+    cta_range_dot<T, VEC>(vals, cols, x, pc.e0, pc.e1, acc, pol);
+    result = (double)block_reduce<T, kBlock>(acc.v, reinterpret_cast<T *>(s_a));
   }
   if (threadIdx.x != 0) return;
   if (pc.npieces == 1) {
@@ -403,6 +474,7 @@ struct csr_args {
   uint32_t lanes;       // CSR vector: lanes per row (power of two, 2..32)
   const uint32_t *__restrict__ row_blocks;  // CSR-Adaptive bins (n_main + 1 entries)
   uint32_t n_main;
+  uint32_t n_pieces;
   const long_piece *__restrict__ pieces;
   double *partials;
   uint32_t *counters;
@@ -458,8 +530,9 @@ __device__ __forceinline__ uint32_t compact_ordered(bool flag, uint32_t value, u
 //           elements rs + l + k*L, then a shuffle tree over the group;
 // and in both, rows above the assist threshold are reduced by a warp.
 template <typename T, int MODE, bool VEC>
-__device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol) {
-  const uint32_t r0 = blockIdx.x * kBlock;
+__device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol,
+                                                  uint32_t blk) {
+  const uint32_t r0 = blk * kBlock;
   const uint32_t nr = min((uint32_t)kBlock, A.n_rows - r0);
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = t; i <= nr; i += kBlock) sm.m.rp[i] = A.row_ptr[r0 + i];
@@ -469,8 +542,11 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
   const uint32_t rs = has ? sm.m.rp[t] : 0u, re = has ? sm.m.rp[t + 1] : 0u;
   const bool is_long = has && (re - rs > A.long_thr);
   const bool is_assist = has && !is_long && (re - rs > A.assist_thr);
-  const uint32_t nlong = compact_ordered<T>(is_long, t, sm.m.longs, sm, &sm.m.nlong);
-  const uint32_t nassist = compact_ordered<T>(is_assist, t, sm.m.assists, sm, &sm.m.nassist);
+  uint32_t nlong = 0, nassist = 0;
+  if (__syncthreads_or(is_long || is_assist)) {
+    nlong = compact_ordered<T>(is_long, t, sm.m.longs, sm, &sm.m.nlong);
+    nassist = compact_ordered<T>(is_assist, t, sm.m.assists, sm, &sm.m.nassist);
+  }
   const uint32_t L = (MODE == 1) ? A.lanes : 1u;
   T acc = T(0);  // scalar: running sum of this thread's row
   uint32_t run_lo = 0;
@@ -486,7 +562,7 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
         if (MODE == 0) {
           if (has && !is_long && !is_assist && t >= run_lo && t < run_hi) {
             const uint32_t lo = max(rs, c0), hi = min(re, c1);
-            for (uint32_t e = lo; e < hi; ++e) acc = add_rn(acc, sm.m.prod[swz(e - base)]);
+            if (lo < hi) acc = seq_sum<T, false>(acc, sm.m.prod, lo - base, hi - base);
           }
         } else {
           const uint32_t G = kBlock / L, g = t / L, gl = t % L;
@@ -501,8 +577,7 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
                 const uint32_t s = max(js, c0), e = min(je, c1);
                 if (s < e) {
                   valid = true;
-                  for (uint32_t i = s + ((gl - (s - js)) & (L - 1u)); i < e; i += L)
-                    part = add_rn(part, sm.m.prod[swz(i - base)]);
+                  part = strided_sum(sm.m.prod, s - base, e - base, (gl - (s - js)) & (L - 1u), L);
                 }
               }
             }
@@ -516,8 +591,7 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
           const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
           const uint32_t s = max(js, c0), e = min(je, c1);
           if (s < e) {
-            T part = T(0);
-            for (uint32_t i = s + ((lane - (s - js)) & 31u); i < e; i += 32) part = add_rn(part, sm.m.prod[swz(i - base)]);
+            T part = strided_sum(sm.m.prod, s - base, e - base, (lane - (s - js)) & 31u, 32u);
             part = group_reduce_down(part, 32);
             if (lane == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
           }
@@ -542,19 +616,19 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
 // reduced by the whole CTA straight from global memory; a single row above
 // the long threshold belongs to pieces.
 template <typename T, bool VEC>
-__device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol) {
-  const uint32_t rb = A.row_blocks[blockIdx.x], re = A.row_blocks[blockIdx.x + 1];
+__device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol,
+                                                  uint32_t blk) {
+  const uint32_t rb = A.row_blocks[blk], re = A.row_blocks[blk + 1];
   const uint32_t nrows = re - rb;
   const uint32_t t = threadIdx.x;
   if (nrows == 0) return;
   const uint32_t a = A.row_ptr[rb], b = A.row_ptr[re];
   if (nrows == 1) {
     if (b - a > A.long_thr) return;
-    T acc = T(0);
-    for (uint32_t e = a + t; e < b; e += kBlock)
-      acc = add_rn(acc, mul_rn(ld_stream1(A.vals + e, pol), ld_x(A.x + ld_stream1(A.cols + e, pol))));
-    acc = block_reduce<T, kBlock>(acc, reinterpret_cast<T *>(sm.p.a));
-    if (t == 0) A.y[rb] = acc;
+    acc_plain<T, VEC> acc;
+    cta_range_dot<T, VEC>(A.vals, A.cols, A.x, a, b, acc, pol);
+    const T r = block_reduce<T, kBlock>(acc.v, reinterpret_cast<T *>(sm.p.a));
+    if (t == 0) A.y[rb] = r;
     return;
   }
   const uint32_t base = a & ~3u;
@@ -569,33 +643,34 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
     const bool valid = grp < nrows;
     if (valid) {
       const uint32_t s = sm.m.rp[grp], e = sm.m.rp[grp + 1];
-      for (uint32_t i = s + lane; i < e; i += tpr) acc = add_rn(acc, sm.m.prod[swz(i - base)]);
+      if (s < e) acc = strided_sum(sm.m.prod, s - base, e - base, lane, tpr);
     }
     acc = group_reduce_down(acc, (int)tpr);
     if (valid && lane == 0) A.y[rb + grp] = acc;
   } else {
     for (uint32_t r = t; r < nrows; r += kBlock) {
       const uint32_t s = A.row_ptr[rb + r], e = A.row_ptr[rb + r + 1];
-      T acc = T(0);
-      for (uint32_t i = s; i < e; ++i) acc = add_rn(acc, sm.m.prod[swz(i - base)]);
-      A.y[rb + r] = acc;
+      A.y[rb + r] = s < e ? seq_sum(T(0), sm.m.prod, s - base, e - base) : T(0);
     }
   }
 }
 
 template <typename T, int ALGO, bool VEC>
-__global__ void __launch_bounds__(kBlock) csr_kernel(const csr_args<T> A) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_CSR_MINBLOCKS : 6) csr_kernel(const csr_args<T> A) {
   __shared__ csr_smem<T> sm;
   const uint64_t pol = policy_evict_first();
-  if (blockIdx.x >= A.n_main) {
-    const long_piece pc = A.pieces[blockIdx.x - A.n_main];
+  // long-row pieces: first block indices (longest work starts first) or last
+  const uint32_t pb = MFP_PIECES_FIRST ? blockIdx.x : blockIdx.x - A.n_main;
+  if (MFP_PIECES_FIRST ? blockIdx.x < A.n_pieces : blockIdx.x >= A.n_main) {
+    const long_piece pc = A.pieces[pb];
     run_piece<T, VEC>(pc, A.vals, A.cols, A.x, A.y, A.partials, A.counters, sm.p.a, sm.p.b, pol);
     return;
   }
+  const uint32_t b = MFP_PIECES_FIRST ? blockIdx.x - A.n_pieces : blockIdx.x;
   if (ALGO == 2)
-    csr_adaptive_main<T, VEC>(A, sm, pol);
+    csr_adaptive_main<T, VEC>(A, sm, pol, b);
   else
-    csr_rowblock_main<T, ALGO, VEC>(A, sm, pol);
+    csr_rowblock_main<T, ALGO, VEC>(A, sm, pol, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -670,7 +745,7 @@ struct coo_smem {
 };
 
 template <typename T, bool VEC>
-__global__ void __launch_bounds__(kBlock) coo_kernel(uint32_t n_rows, uint32_t nnz,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uint32_t n_rows, uint32_t nnz,
                                                      const T *__restrict__ vals,
                                                      const uint32_t *__restrict__ cols,
                                                      const uint32_t *__restrict__ rows,
@@ -787,7 +862,7 @@ struct scoo_smem_static {
 };
 
 template <typename T, bool VEC, bool XWIN>
-__global__ void __launch_bounds__(kBlock) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,
                                                       const uint32_t *__restrict__ ridx,
@@ -851,7 +926,7 @@ struct hyb_smem {
 };
 
 template <typename T, bool VEC>
-__global__ void __launch_bounds__(kBlock) hyb_kernel(uint32_t n_rows, uint32_t width,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) hyb_kernel(uint32_t n_rows, uint32_t width,
                                                      const T *__restrict__ ell_data,
                                                      const uint32_t *__restrict__ ell_cols,
                                                      const T *__restrict__ coo_data,

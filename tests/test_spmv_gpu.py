@@ -129,8 +129,11 @@ def test_scalar_and_ell_exact_on_laplacian_512(oracle_lib, dt):
     m = syn("laplacian_512").astype(dt)
     x = synth.vector(0, m.cols).astype(dt)
     y_ref = oracle_lib.csr_spmv(m.rows, m.row_ptr, m.columns, m.data, x)
-    assert np.array_equal(run(m, CSR_SCALAR, x), y_ref)  # rows of 5: default config is exact too
+    assert np.array_equal(run(m, CSR_SCALAR, x, EXACT_SCALAR), y_ref)
     assert np.array_equal(run(m, ELL, x), y_ref)
+    # default (streaming) configuration: exact except rows split between two CTA ranges
+    y = run(m, CSR_SCALAR, x)
+    assert np.count_nonzero(y != y_ref) <= 2 * 148 * 8
 
 
 def _long_rows_matrix(dt):
@@ -282,3 +285,35 @@ def test_full_size_power_law_float32(oracle_lib, fmt):
     # size-independent checksum: sum_i y_i = sum_j (column sum of A)_j x_j
     colsum = np.bincount(m.columns, weights=m.data.astype(np.float64), minlength=m.cols)
     assert abs(y.astype(np.float64).sum() - colsum @ x.astype(np.float64)) < 1e-3 * np.abs(m.data).sum() ** 0.5
+
+
+STREAM_CASES = ["laplacian_16", "powerlaw_small", "edge_long_row", "edge_empty_rows", "random_rect"]
+
+
+@pytest.mark.parametrize("kernel", [2, 3])
+@pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE])
+@pytest.mark.parametrize("s", ["f32", "f64"])
+def test_streaming_csr_kernel(oracle_lib, kernel, fmt, s):
+    """The streaming CSR kernel (persistent CTAs, TMA chunks) on fixtures, synthetic and long-row matrices."""
+    cfg = {"kernel": kernel}
+    for case in STREAM_CASES:
+        g = load_golden(case)
+        m = golden_csr(g, s)
+        x = g["x"].astype(m.dtype)
+        check_tol(oracle_lib, m, x, run(m, fmt, x, cfg), f"stream{kernel} {case}/{s}/fmt{fmt}")
+    dt = np.float32 if s == "f32" else np.float64
+    for m in (syn("power_law_300k").astype(dt), _long_rows_matrix(dt), syn("uniform_rect").astype(dt)):
+        x = synth.vector(6, m.cols).astype(dt)
+        ys = run(m, fmt, x, cfg, reps=2)
+        check_tol(oracle_lib, m, x, ys[0], f"stream{kernel} synthetic fmt{fmt}")
+        assert np.array_equal(ys[0], ys[1])
+
+
+@pytest.mark.parametrize("kernel", [2, 3])
+def test_streaming_scalar_exact_within_cta_ranges(oracle_lib, kernel):
+    """Scalar streaming keeps CSR order (exact) except rows split between CTA ranges."""
+    m = syn("laplacian_512").astype(np.float32)
+    x = synth.vector(0, m.cols).astype(np.float32)
+    y_ref = oracle_lib.csr_spmv(m.rows, m.row_ptr, m.columns, m.data, x)
+    y = run(m, CSR_SCALAR, x, {"kernel": kernel, "assist_threshold": NEVER})
+    assert np.count_nonzero(y != y_ref) <= 2 * 148 * 8
