@@ -207,6 +207,23 @@ int mfp_coo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t nnz, const double *d
 /* Reads the workspace's error word (non-zero: a bounded wait gave up). Synchronous. */
 int mfp_workspace_error(const void *workspace, uint32_t *error);
 
+/* COO SpMV (float) that allocates nothing.  No counterpart in the reference:
+ * it serves callers that may not allocate device memory themselves (hosts
+ * that own every byte through their own pool or budget, or loops that cannot
+ * take cudaMalloc's latency and implicit synchronisation).  Same arguments and
+ * result as mfp_coo_spmv_f32 without the workspace: the look-back scratch is a
+ * fixed 1 MiB array inside the library, present on every device that loads
+ * it, so nnz is limited to 134,215,680 (larger -> MFP_ERROR_TOO_LARGE).
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call clears the part of the array it uses with cudaMemsetAsync on
+ * `stream`; all calls share the one array, so calls that overlap on the GPU
+ * (different streams, or different host threads) race and must not be issued
+ * concurrently. */
+int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
+                             const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
+                             void *stream);
+
 /* SCOO — counterpart of gpu_scoo_spmv (gpu/scoo_spmv.cu:46-222).  One CTA per
  * slice.  x_windows (device, 2 uint32 per slice: first and one-past-last
  * column of the slice, from mfp_scoo_x_windows) lets a slice stage its x

@@ -1046,3 +1046,53 @@ int mfp_matrix_time(const mfp_matrix *m, const void *x, void *y, uint32_t reps, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// COO SpMV that allocates nothing (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+// Some callers cannot let a library call cudaMalloc: hosts that hand out all
+// device memory through their own pool or budget, and loops that cannot
+// afford cudaMalloc's latency and implicit synchronisation.  This entry point
+// keeps the COO look-back workspace in a fixed array that is part of the
+// library image instead.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB on every device that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 64;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (host code cannot
+// use the array's name as an address).  Resolved once per device.
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(MFP_ERROR_NOT_SUPPORTED, "device %d beyond %d", dev, kMaxDevices);
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return MFP_SUCCESS;
+}
+}  // namespace
+
+extern "C" int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
+                                        const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
+                                        void *stream) {
+  const size_t need = coo_ws_bytes(nnz);
+  if (need > kNoAllocScratchBytes)
+    return fail(MFP_ERROR_TOO_LARGE,
+                "nnz %u needs %zu bytes of COO scratch; the fixed scratch holds %zu bytes (nnz <= %zu)", nnz, need,
+                kNoAllocScratchBytes,
+                (kNoAllocScratchBytes - sizeof(d::coo_ws_header)) / sizeof(d::coo_tile_state<double>) * d::kChunk);
+  void *ws = nullptr;
+  int st = noalloc_scratch(&ws);
+  if (st) return st;
+  // the workspace must start zeroed; the previous call's contents are cleared on this stream
+  if (rows && nnz) CUDA_TRY(cudaMemsetAsync(ws, 0, need, as_stream(stream)), "cudaMemsetAsync(scratch)");
+  return coo_spmv<float>(rows, nnz, data, col_ids, row_ids, x, y, ws, need, stream);
+}
