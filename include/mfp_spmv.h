@@ -241,23 +241,20 @@ int mfp_scoo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t slices_count, uint3
                       const double *x, double *y, void *stream);
 
 /* Hybrid ELL + COO — counterpart of gpu_hybrid_spmv / gpu_hybrid_atomic_spmv
- * (gpu_matrix_multiplier.cu:866-1096).  One kernel: each CTA owns
- * MFP_HYB_ROWS_PER_BLOCK rows, adds their ELL slots and their COO-tail
- * elements, and writes each y once (no atomics).  tail_block_ptr (device,
- * ceil(rows / MFP_HYB_ROWS_PER_BLOCK) + 1 entries) is the first tail element
- * of each row block, from mfp_hybrid_tail_block_ptr on the host tail rows. */
-#define MFP_HYB_ROWS_PER_BLOCK 1024u
-int mfp_hybrid_tail_block_ptr(uint32_t rows, uint32_t coo_nnz, const uint32_t *coo_rows,
-                              uint32_t *tail_block_ptr);
+ * (gpu_matrix_multiplier.cu:866-1096).  Two launches: the ELL kernel writes
+ * every row's ELL part, then the tile-based COO kernel adds the tail (the
+ * elements past the ELL width, hybrid_matrix_class's coo_matrix) row by row,
+ * without atomics.  `workspace` is the COO look-back workspace of the tail
+ * (mfp_hybrid_workspace_bytes; zero-filled before first use, left zeroed). */
+int mfp_hybrid_workspace_bytes(uint32_t rows, uint32_t coo_nnz, size_t *bytes);
 int mfp_hybrid_spmv_f32(uint32_t rows, uint32_t cols, uint32_t ell_width, const float *ell_data,
                         const uint32_t *ell_cols, uint32_t coo_nnz, const float *coo_data,
-                        const uint32_t *coo_cols, const uint32_t *coo_rows,
-                        const uint32_t *tail_block_ptr, const float *x, float *y, void *stream);
+                        const uint32_t *coo_cols, const uint32_t *coo_rows, const float *x, float *y,
+                        void *workspace, size_t workspace_bytes, void *stream);
 int mfp_hybrid_spmv_f64(uint32_t rows, uint32_t cols, uint32_t ell_width, const double *ell_data,
                         const uint32_t *ell_cols, uint32_t coo_nnz, const double *coo_data,
-                        const uint32_t *coo_cols, const uint32_t *coo_rows,
-                        const uint32_t *tail_block_ptr, const double *x, double *y,
-                        void *stream);
+                        const uint32_t *coo_cols, const uint32_t *coo_rows, const double *x, double *y,
+                        void *workspace, size_t workspace_bytes, void *stream);
 
 /* fill_vector — gpu_matrix_multiplier.cu:45-52. */
 int mfp_fill_f32(uint64_t n, float *vec, float value, void *stream);

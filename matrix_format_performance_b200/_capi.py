@@ -96,9 +96,9 @@ _PROTOS = {
     "mfp_scoo_x_windows": [u32, vp, vp, u32, vp],
     "mfp_scoo_spmv_f32": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp],
     "mfp_scoo_spmv_f64": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp],
-    "mfp_hybrid_tail_block_ptr": [u32, u32, vp, vp],
-    "mfp_hybrid_spmv_f32": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp],
-    "mfp_hybrid_spmv_f64": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp],
+    "mfp_hybrid_workspace_bytes": [u32, u32, C.POINTER(C.c_size_t)],
+    "mfp_hybrid_spmv_f32": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],
+    "mfp_hybrid_spmv_f64": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],
     "mfp_fill_f32": [u64, vp, C.c_float, vp],
     "mfp_fill_f64": [u64, vp, f64, vp],
     "mfp_matrix_create_csr": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(CsrConfig), C.POINTER(vp)],

@@ -480,12 +480,12 @@ size_t coo_ws_bytes(uint32_t nnz) {
   return sizeof(d::coo_ws_header) + tiles * sizeof(d::coo_tile_state<double>);
 }
 
-template <typename T>
+template <typename T, bool ACCUM = false>
 int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
              const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
   if (rows == 0) return ok();
   if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
-  if (nnz == 0) return fill<T>(rows, y, T(0), stream);
+  if (nnz == 0) return ACCUM ? ok() : fill<T>(rows, y, T(0), stream);
   if (!data || !cols || !rids || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   if (!ws || ws_bytes < coo_ws_bytes(nnz))
     return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_ws_bytes(nnz), ws_bytes);
@@ -496,9 +496,9 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
   cudaStream_t s = as_stream(stream);
   if (vec)
-    d::coo_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+    d::coo_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
   else
-    d::coo_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+    d::coo_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
   return check_launch("coo_kernel launch");
 }
 
@@ -552,20 +552,17 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
   return scoo_launch<T, false, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
 }
 
+// Hybrid: the ELL kernel writes every row's ELL part, then the tile-based COO
+// kernel adds the tail (elements past the ELL width) row by row.
 template <typename T>
 int hyb_spmv(uint32_t rows, uint32_t width, const T *ed, const uint32_t *ec, uint32_t cnnz, const T *cd,
-             const uint32_t *cc, const uint32_t *cr, const uint32_t *tp, const T *x, T *y, void *stream) {
+             const uint32_t *cc, const uint32_t *cr, const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
   if (rows == 0) return ok();
-  if (!y || !x || !tp || (width && (!ed || !ec)) || (cnnz && (!cd || !cc || !cr)))
+  if (!y || !x || (width && (!ed || !ec)) || (cnnz && (!cd || !cc || !cr)))
     return fail(MFP_ERROR_INVALID_VALUE, "null device array");
-  const bool vec = (rows % 4 == 0) && aligned16(ed) && aligned16(ec) && aligned16(cd) && aligned16(cc) && aligned16(cr);
-  const uint32_t grid = ceil_div(rows, d::kHybRows);
-  cudaStream_t s = as_stream(stream);
-  if (vec)
-    d::hyb_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, width, ed, ec, cd, cc, cr, tp, x, y);
-  else
-    d::hyb_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, width, ed, ec, cd, cc, cr, tp, x, y);
-  return check_launch("hyb_kernel launch");
+  int st = ell_spmv<T>(rows, width, ed, ec, x, y, stream);
+  if (st) return st;
+  return coo_spmv<T, true>(rows, cnnz, cd, cc, cr, x, y, ws, ws_bytes, stream);
 }
 }  // namespace
 
@@ -632,15 +629,20 @@ int mfp_scoo_spmv_f64(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, 
                       double *y, void *s) {
   return scoo_spmv<double>(rows, slices, slice, v, ci, ri, sp, win, maxw, x, y, s);
 }
+int mfp_hybrid_workspace_bytes(uint32_t rows, uint32_t coo_nnz, size_t *bytes) {
+  if (!bytes) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *bytes = coo_ws_bytes(coo_nnz);
+  return ok();
+}
 int mfp_hybrid_spmv_f32(uint32_t rows, uint32_t, uint32_t w, const float *ed, const uint32_t *ec, uint32_t cn,
-                        const float *cd, const uint32_t *cc, const uint32_t *cr, const uint32_t *tp, const float *x,
-                        float *y, void *s) {
-  return hyb_spmv<float>(rows, w, ed, ec, cn, cd, cc, cr, tp, x, y, s);
+                        const float *cd, const uint32_t *cc, const uint32_t *cr, const float *x, float *y, void *ws,
+                        size_t wsb, void *s) {
+  return hyb_spmv<float>(rows, w, ed, ec, cn, cd, cc, cr, x, y, ws, wsb, s);
 }
 int mfp_hybrid_spmv_f64(uint32_t rows, uint32_t, uint32_t w, const double *ed, const uint32_t *ec, uint32_t cn,
-                        const double *cd, const uint32_t *cc, const uint32_t *cr, const uint32_t *tp,
-                        const double *x, double *y, void *s) {
-  return hyb_spmv<double>(rows, w, ed, ec, cn, cd, cc, cr, tp, x, y, s);
+                        const double *cd, const uint32_t *cc, const uint32_t *cr, const double *x, double *y,
+                        void *ws, size_t wsb, void *s) {
+  return hyb_spmv<double>(rows, w, ed, ec, cn, cd, cc, cr, x, y, ws, wsb, s);
 }
 int mfp_fill_f32(uint64_t n, float *v, float value, void *s) { return fill<float>(n, v, value, s); }
 int mfp_fill_f64(uint64_t n, double *v, double value, void *s) { return fill<double>(n, v, value, s); }
@@ -661,7 +663,7 @@ struct mfp_matrix {
   void *vals = nullptr;
   uint32_t *cols_a = nullptr;
   uint32_t *rows_a = nullptr;   // CSR row_ptr, COO/SCOO row ids
-  uint32_t *aux = nullptr;      // SCOO slices_ptr, HYB tail block ptr
+  uint32_t *aux = nullptr;      // SCOO slices_ptr
   uint32_t *win = nullptr;      // SCOO x windows
   void *vals2 = nullptr;        // HYB COO tail
   uint32_t *cols2 = nullptr, *rows2 = nullptr;
@@ -915,17 +917,20 @@ int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t widt
     nz += !(zero && ec[i] == 0);
   }
   m->nnz = nz + cnnz;
-  const uint32_t nb = ceil_div(rows, MFP_HYB_ROWS_PER_BLOCK);
-  std::vector<uint32_t> tp((size_t)nb + 1);
-  mfp_hybrid_tail_block_ptr(rows, cnnz, cr, tp.data());
-  m->format_bytes = slots * (vs + 4) + (uint64_t)cnnz * (vs + 8) + ((uint64_t)nb + 1) * 4 + (uint64_t)cols * vs +
-                    (uint64_t)rows * vs;
+  m->format_bytes = slots * (vs + 4) + (uint64_t)cnnz * (vs + 8) + (uint64_t)cols * vs + (uint64_t)rows * vs;
+  m->ws_bytes = coo_ws_bytes(cnnz);
+  unsigned char *ws = nullptr;
   int st;
   if ((st = track_upload_bytes(m, &m->vals, ed, slots * vs)) || (st = track_upload(m, &m->cols_a, ec, slots)) ||
       (st = track_upload_bytes(m, &m->vals2, cd, (size_t)cnnz * vs)) || (st = track_upload(m, &m->cols2, cc, cnnz)) ||
-      (st = track_upload(m, &m->rows2, cr, cnnz)) || (st = track_upload(m, &m->aux, tp.data(), tp.size()))) {
+      (st = track_upload(m, &m->rows2, cr, cnnz)) || (st = track(m, &ws, m->ws_bytes))) {
     mfp_matrix_destroy(m);
     return st;
+  }
+  m->ws = ws;
+  if (ws && cudaMemset(ws, 0, m->ws_bytes) != cudaSuccess) {
+    mfp_matrix_destroy(m);
+    return fail(MFP_ERROR_CUDA, "cudaMemset workspace");
   }
   return finish_matrix(m, out);
 }
@@ -941,7 +946,7 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
   out->format_bytes = m->format_bytes;
   out->algorithmic_bytes = m->nnz * (vs + 4) + ((uint64_t)m->rows + 1) * 4 + (uint64_t)m->cols * vs + (uint64_t)m->rows * vs;
   out->device_bytes = m->device_bytes;
-  out->kernel_launches = 1;
+  out->kernel_launches = (m->format == MFP_FORMAT_HYBRID && m->coo_nnz) ? 2 : 1;
   return ok();
 }
 
@@ -973,11 +978,11 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                                     m->aux, m->win, m->max_window, (const float *)x, (float *)y, stream);
     case MFP_FORMAT_HYBRID:
       return f64 ? hyb_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, m->coo_nnz,
-                                    (const double *)m->vals2, m->cols2, m->rows2, m->aux, (const double *)x,
-                                    (double *)y, stream)
+                                    (const double *)m->vals2, m->cols2, m->rows2, (const double *)x, (double *)y,
+                                    m->ws, m->ws_bytes, stream)
                  : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
-                                   (const float *)m->vals2, m->cols2, m->rows2, m->aux, (const float *)x, (float *)y,
-                                   stream);
+                                   (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
+                                   m->ws_bytes, stream);
     default:
       return fail(MFP_ERROR_INVALID_VALUE, "unknown format %d", m->format);
   }

@@ -379,15 +379,4 @@ int mfp_scoo_x_windows(uint32_t nnz, const uint32_t *ci, const uint32_t *sp, uin
   return ok();
 }
 
-int mfp_hybrid_tail_block_ptr(uint32_t rows, uint32_t nnz, const uint32_t *cr, uint32_t *tp) {
-  if (!tp || (nnz && !cr)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
-  const uint32_t nb = (rows + MFP_HYB_ROWS_PER_BLOCK - 1) / MFP_HYB_ROWS_PER_BLOCK;
-  for (uint32_t b = 0; b <= nb; ++b) {
-    const uint64_t r = (uint64_t)b * MFP_HYB_ROWS_PER_BLOCK;
-    tp[b] = (uint32_t)(std::lower_bound(cr, cr + nnz, (uint32_t)std::min<uint64_t>(r, UINT32_MAX)) - cr);
-    if (r >= rows) tp[b] = nnz;
-  }
-  return ok();
-}
-
 }  // extern "C"

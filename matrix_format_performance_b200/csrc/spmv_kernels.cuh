@@ -20,8 +20,10 @@
 //   SCOO          one CTA per slice, shared-memory row accumulators and an
 //                 optional shared-memory copy of the slice's x window
 //                 (gpu/scoo_spmv.cu:46-129)
-//   HYB           one CTA per row block: ELL slots plus the block's COO tail
-//                 (gpu/gpu_matrix_multiplier.cu:969-1002)
+//   HYB           the ELL kernel for the ELL part, then the COO kernel in
+//                 accumulate mode for the tail (two launches, as the
+//                 reference's gpu/gpu_matrix_multiplier.cu:969-1002, with
+//                 the tail's atomics replaced by the COO tile reduction)
 // Rows longer than a plan threshold (CSR family) are cut into pieces that
 // run as extra CTAs of the same launch and meet in a partial-sum buffer.
 #pragma once
@@ -565,12 +567,29 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
             if (lo < hi) acc = seq_sum<T, false>(acc, sm.m.prod, lo - base, hi - base);
           }
         } else {
+          // rows of the run that intersect [c0, c1): [jlo, jhi), by binary search
+          uint32_t jlo, jhi;
+          {
+            uint32_t lo_ = run_lo, hi_ = run_hi;  // first j with rp[j + 1] > c0
+            while (lo_ < hi_) {
+              const uint32_t mid = (lo_ + hi_) >> 1;
+              if (sm.m.rp[mid + 1] > c0) hi_ = mid; else lo_ = mid + 1;
+            }
+            jlo = lo_;
+            hi_ = run_hi;  // first j with rp[j] >= c1
+            while (lo_ < hi_) {
+              const uint32_t mid = (lo_ + hi_) >> 1;
+              if (sm.m.rp[mid] >= c1) hi_ = mid; else lo_ = mid + 1;
+            }
+            jhi = lo_;
+          }
           const uint32_t G = kBlock / L, g = t / L, gl = t % L;
-          for (uint32_t it = 0; it < L; ++it) {
-            const uint32_t j = g + it * G;
+          const uint32_t rounds = (jhi - jlo + G - 1u) / G;  // uniform over the CTA
+          for (uint32_t it = 0; it < rounds; ++it) {
+            const uint32_t j = jlo + g + it * G;
             T part = T(0);
             bool valid = false;
-            if (j < nr && j >= run_lo && j < run_hi) {
+            if (j < jhi) {
               const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
               const uint32_t len = je - js;
               if (len <= A.assist_thr) {
@@ -656,7 +675,7 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
 }
 
 template <typename T, int ALGO, bool VEC>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_CSR_MINBLOCKS : 6) csr_kernel(const csr_args<T> A) {
+__global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && ALGO != 1) ? MFP_CSR_MINBLOCKS : 6) csr_kernel(const csr_args<T> A) {
   __shared__ csr_smem<T> sm;
   const uint64_t pol = policy_evict_first();
   // long-row pieces: first block indices (longest work starts first) or last
@@ -744,7 +763,10 @@ struct coo_smem {
   uint32_t first_row, last_row;
 };
 
-template <typename T, bool VEC>
+// ACCUM: add each row's total to y instead of storing it, and leave rows
+// without elements untouched (the COO tail of the hybrid format, after the
+// ELL kernel has written every row).
+template <typename T, bool VEC, bool ACCUM = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uint32_t n_rows, uint32_t nnz,
                                                      const T *__restrict__ vals,
                                                      const uint32_t *__restrict__ cols,
@@ -779,7 +801,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
   const uint32_t off = c0 - base, n = c1 - c0;
   const uint32_t rf = sm.row[swz(off)], rl = sm.row[swz(off + n - 1)];
   // empty rows before the first row of this tile (after the previous tile's last)
-  {
+  if (!ACCUM) {
     const uint32_t lo = (p == kNoRow) ? 0u : p + 1u;
     for (uint32_t r = lo + threadIdx.x; r < rf && r < n_rows; r += kBlock) y[r] = T(0);
     if (c1 == nnz)
@@ -789,14 +811,15 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
     const bool cont_prev = is_first && row == p;
     const bool cont_next = is_last && row == nx;
     if (!cont_prev && !cont_next) {
-      if (row < n_rows) y[row] = total;
+      if (row < n_rows) y[row] = ACCUM ? add_rn(y[row], total) : total;
       return;
     }
     if (is_first) sm.first_total = total;
     if (is_last) sm.last_total = total;
   };
   auto gap = [&](uint32_t lo, uint32_t hi) {
-    for (uint32_t r = lo; r < hi && r < n_rows; ++r) y[r] = T(0);
+    if (!ACCUM)
+      for (uint32_t r = lo; r < hi && r < n_rows; ++r) y[r] = T(0);
   };
   block_segmented_reduce<T>(sm.prod, sm.row, off, n, emit, gap, sm.scan);
   __syncthreads();
@@ -839,7 +862,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
         if (kind != 2u) break;
       }
       if (!ok) atomicOr(&ws->error, 1u);
-      if (rf < n_rows) y[rf] = add_rn(sum, sm.first_total);
+      if (rf < n_rows) y[rf] = ACCUM ? add_rn(y[rf], add_rn(sum, sm.first_total)) : add_rn(sum, sm.first_total);
     }
     __threadfence();
     const uint32_t d = atomicAdd(&ws->done, 1u);
@@ -912,76 +935,6 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) scoo_kernel(ui
   for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
 }
 
-// ---------------------------------------------------------------------------
-// HYB: CTA b owns rows [b*1024, b*1024+1024): 4 rows per thread over the ELL
-// slots, then the block's COO-tail elements [tail_ptr[b], tail_ptr[b+1]).
-// ---------------------------------------------------------------------------
-constexpr uint32_t kHybRows = 1024;
-template <typename T>
-struct hyb_smem {
-  __align__(16) T acc[kHybRows];
-  __align__(16) T prod[kChunkPad];
-  __align__(16) uint32_t row[kChunkPad];
-  seg_scan_smem<T> scan;
-};
-
-template <typename T, bool VEC>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) hyb_kernel(uint32_t n_rows, uint32_t width,
-                                                     const T *__restrict__ ell_data,
-                                                     const uint32_t *__restrict__ ell_cols,
-                                                     const T *__restrict__ coo_data,
-                                                     const uint32_t *__restrict__ coo_cols,
-                                                     const uint32_t *__restrict__ coo_rows,
-                                                     const uint32_t *__restrict__ tail_ptr,
-                                                     const T *__restrict__ x, T *__restrict__ y) {
-  __shared__ hyb_smem<T> sm;
-  const uint64_t pol = policy_evict_first();
-  const uint32_t r0 = blockIdx.x * kHybRows;
-  const uint32_t nr = min(kHybRows, n_rows - r0);
-  const size_t stride = n_rows;
-  if (VEC) {  // n_rows % 4 == 0
-    const uint32_t lr = threadIdx.x * 4u;
-    if (lr < nr) {
-      T a[4] = {T(0), T(0), T(0), T(0)};
-      for (uint32_t k = 0; k < width; ++k) {
-        T v[4];
-        uint32_t c[4];
-        ld_stream4(ell_data + k * stride + r0 + lr, v, pol);
-        ld_stream4(ell_cols + k * stride + r0 + lr, c, pol);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) a[j] = add_rn(a[j], mul_rn(v[j], ld_x(x + c[j])));
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) sm.acc[lr + j] = a[j];
-    }
-  } else {
-    for (uint32_t lr = threadIdx.x; lr < nr; lr += kBlock) {
-      T a = T(0);
-      for (uint32_t k = 0; k < width; ++k) {
-        const size_t o = k * stride + r0 + lr;
-        a = add_rn(a, mul_rn(ld_stream1(ell_data + o, pol), ld_x(x + ld_stream1(ell_cols + o, pol))));
-      }
-      sm.acc[lr] = a;
-    }
-  }
-  __syncthreads();
-  const uint32_t tb = tail_ptr[blockIdx.x], te = tail_ptr[blockIdx.x + 1];
-  auto emit = [&](uint32_t row, T total, bool, bool) {
-    const uint32_t lr = row - r0;
-    if (lr < nr) sm.acc[lr] = add_rn(sm.acc[lr], total);
-  };
-  auto gap = [](uint32_t, uint32_t) {};
-  for (uint32_t c0 = tb; c0 < te;) {
-    const uint32_t base = c0 & ~3u;
-    const uint32_t c1 = min(te, base + (uint32_t)kChunk);
-    stage<T, VEC, true>(coo_data, coo_cols, coo_rows, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
-    __syncthreads();
-    block_segmented_reduce<T>(sm.prod, sm.row, c0 - base, c1 - c0, emit, gap, sm.scan);
-    __syncthreads();
-    c0 = c1;
-  }
-  for (uint32_t i = threadIdx.x; i < nr; i += kBlock) y[r0 + i] = sm.acc[i];
-}
 
 template <typename T>
 __global__ void fill_kernel(uint64_t n, T *v, T value) {
