@@ -45,7 +45,9 @@ typedef enum mfp_status {
   MFP_ERROR_DEVICE_WAIT = 6     /* a bounded device-side wait gave up */
 } mfp_status;
 
-typedef enum mfp_value_type { MFP_F32 = 0, MFP_F64 = 1 } mfp_value_type;
+/* MFP_BF16 / MFP_F16: 16-bit stored values of the reduced-precision CSR
+ * layout (x, y and the accumulation stay FP32). */
+typedef enum mfp_value_type { MFP_F32 = 0, MFP_F64 = 1, MFP_BF16 = 2, MFP_F16 = 3 } mfp_value_type;
 
 /* ------------------------------------------------------------------------- */
 /* Library                                                                   */
@@ -256,6 +258,35 @@ int mfp_hybrid_spmv_f64(uint32_t rows, uint32_t cols, uint32_t ell_width, const 
                         const uint32_t *coo_cols, const uint32_t *coo_rows, const double *x, double *y,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- Reduced-precision CSR (engine extension; the reference has float and
+ * double CSR only, gpu_matrix_multiplier.cu:54-129) -------------------------
+ * Layout: row_ptr[rows + 1] uint32 as CSR; q[nnz] uint16 bit patterns of
+ * round(a_ij / scale_i) in BF16 or FP16; scale[rows] float, scale_i =
+ * max_j |a_ij| (1 for an empty or all-zero row); columns[nnz] uint32, or
+ * delta[nnz] uint16 with column = base[e / MFP_LOWP_DELTA_CHUNK] + delta[e].
+ * y_i = scale_i * sum_j float(q_ij) * x_j with FP32 accumulation. */
+#define MFP_LOWP_DELTA_CHUNK 2048u
+
+/* Host quantizer: q and scale from FP64 values (a_ij / scale_i rounded to
+ * FP32, then to BF16 or FP16 with round-to-nearest-even). */
+int mfp_lowp_quantize(int value_type, uint32_t rows, const uint32_t *row_ptr, const double *values,
+                      uint16_t *q, float *scale);
+/* Host delta encoder: base[k] = smallest column of chunk k, delta = column -
+ * base; MFP_ERROR_NOT_SUPPORTED if a chunk's span exceeds 65535. */
+int mfp_lowp_deltas(uint32_t nnz, const uint32_t *columns, uint16_t *delta, uint32_t *base);
+/* y = A*x for that layout (device arrays); columns (uint32) or delta + base
+ * (16-bit) is given, the other null.  With q, the indices and row_ptr
+ * 16-byte aligned the launch is the pipelined kernel (TMA bulk copies into
+ * shared-memory stages); otherwise a row-block kernel with plain loads.  Both
+ * are within FP32 rounding of each other (their sum orders differ). */
+int mfp_lowp_spmv(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row_ptr,
+                  const uint16_t *q, const float *scale, const uint32_t *columns, const uint16_t *delta,
+                  const uint32_t *base, const float *x, float *y, void *stream);
+/* Error word of the pipelined reduced-precision kernel on `device` (bit 0: a
+ * stage wait gave up, the results of that launch are incomplete); `clear`
+ * resets it.  Synchronous.  Engine extension, no counterpart in the reference. */
+int mfp_lowp_error(int device, int clear, uint32_t *error);
+
 /* fill_vector — gpu_matrix_multiplier.cu:45-52. */
 int mfp_fill_f32(uint64_t n, float *vec, float value, void *stream);
 int mfp_fill_f64(uint64_t n, double *vec, double value, void *stream);
@@ -275,7 +306,8 @@ typedef enum mfp_format {
   MFP_FORMAT_ELL = 3,
   MFP_FORMAT_COO = 4,
   MFP_FORMAT_SCOO = 5,
-  MFP_FORMAT_HYBRID = 6
+  MFP_FORMAT_HYBRID = 6,
+  MFP_FORMAT_CSR_LOWP = 7 /* reduced-precision CSR (engine extension) */
 } mfp_format;
 typedef struct mfp_matrix mfp_matrix;
 
@@ -296,6 +328,12 @@ int mfp_matrix_create_hybrid(int value_type, uint32_t rows, uint32_t cols, uint3
                              const uint32_t *ell_columns, const void *ell_data, uint32_t coo_nnz,
                              const uint32_t *coo_rows, const uint32_t *coo_cols,
                              const void *coo_data, mfp_matrix **out);
+/* Reduced-precision CSR from host CSR with FP64 values: quantized on the host
+ * (mfp_lowp_quantize), 16-bit column deltas when index16 != 0 and every
+ * 2048-element chunk's column span fits 16 bits (else MFP_ERROR_NOT_SUPPORTED). */
+int mfp_matrix_create_lowp(int value_type, int index16, uint32_t rows, uint32_t cols, uint32_t nnz,
+                           const uint32_t *row_ptr, const uint32_t *columns, const double *values,
+                           mfp_matrix **out);
 int mfp_matrix_destroy(mfp_matrix *m);
 
 typedef struct mfp_matrix_info {

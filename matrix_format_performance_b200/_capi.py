@@ -99,6 +99,11 @@ _PROTOS = {
     "mfp_hybrid_workspace_bytes": [u32, u32, C.POINTER(C.c_size_t)],
     "mfp_hybrid_spmv_f32": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],
     "mfp_hybrid_spmv_f64": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],
+    "mfp_lowp_quantize": [i32, u32, vp, vp, vp, vp],
+    "mfp_lowp_deltas": [u32, vp, vp, vp],
+    "mfp_lowp_spmv": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp],
+    "mfp_lowp_error": [i32, i32, P_u32],
+    "mfp_matrix_create_lowp": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(vp)],
     "mfp_fill_f32": [u64, vp, C.c_float, vp],
     "mfp_fill_f64": [u64, vp, f64, vp],
     "mfp_matrix_create_csr": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(CsrConfig), C.POINTER(vp)],

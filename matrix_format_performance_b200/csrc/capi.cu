@@ -2,10 +2,13 @@
 #include "host_common.h"
 #include "spmv_kernels.cuh"
 #include "spmv_stream.cuh"
+#include "spmv_lowp.cuh"
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 using namespace mfp;
@@ -29,6 +32,60 @@ inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1)
 int check_launch(const char *what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what);
+  return ok();
+}
+
+// Per (kernel, device): the dynamic shared-memory limit set so far and the
+// resident CTAs per SM of a persistent launch.
+struct kernel_cache {
+  std::mutex mu;
+  std::map<std::pair<const void *, int>, size_t> limit;
+  std::map<std::pair<const void *, int>, int> occupancy;
+  std::map<int, int> sms;
+};
+kernel_cache &kcache() {
+  static kernel_cache c;
+  return c;
+}
+
+// Raises `k`'s dynamic shared-memory limit on the current device to `dyn`.
+int ensure_dyn_smem(const void *k, size_t dyn, const char *name) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+  auto &c = kcache();
+  std::lock_guard<std::mutex> g(c.mu);
+  size_t &lim = c.limit[{k, dev}];
+  if (dyn <= lim) return ok();
+  const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MFP_ERROR_CUDA, "cudaFuncSetAttribute(%s, %zu dynamic bytes): %s", name, dyn, cudaGetErrorString(e));
+  }
+  lim = dyn;
+  return ok();
+}
+
+// Resident CTAs per SM of `k` (block `threads`, `dyn` dynamic bytes) times the
+// SM count of the current device: the grid of a persistent launch.
+int persistent_grid(const void *k, int threads, size_t dyn, uint32_t *grid) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+  auto &c = kcache();
+  std::lock_guard<std::mutex> g(c.mu);
+  auto it = c.occupancy.find({k, dev});
+  if (it == c.occupancy.end()) {
+    int blocks = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, threads, dyn),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    it = c.occupancy.emplace(std::make_pair(k, dev), std::max(1, blocks)).first;
+  }
+  auto sit = c.sms.find(dev);
+  if (sit == c.sms.end()) {
+    int n = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    sit = c.sms.emplace(dev, n).first;
+  }
+  *grid = (uint32_t)it->second * (uint32_t)sit->second;
   return ok();
 }
 
@@ -507,20 +564,9 @@ int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32
                 const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
                 const T *x, T *y) {
   auto k = d::scoo_kernel<T, VEC, XWIN>;
-  // raise the kernel's dynamic shared-memory limit when a launch needs more
-  static std::mutex mu;
-  static size_t limit = 0;
-  {
-    std::lock_guard<std::mutex> g(mu);
-    if (dyn > limit && dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
-      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(MFP_ERROR_CUDA, "cudaFuncSetAttribute(scoo_kernel, %zu dynamic bytes, %zu static): %s", dyn,
-                    sizeof(d::scoo_smem_static<T>), cudaGetErrorString(e));
-      }
-      limit = dyn;
-    }
+  if (dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
+    const int st = ensure_dyn_smem((const void *)k, dyn, "scoo_kernel");
+    if (st) return st;
   }
   k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, x, y);
   const cudaError_t e = cudaGetLastError();
@@ -550,6 +596,80 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
   }
   if (win) return scoo_launch<T, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
   return scoo_launch<T, false, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, x, y);
+}
+
+// Pipelined reduced-precision kernel: CAP elements per stage, S stages.  A
+// stage of the defaults holds a 256-row block of up to 32 elements per row
+// (16-bit indices) in about 35 KB; three CTAs share an SM.
+#ifndef MFP_LOWP_CAP16
+#define MFP_LOWP_CAP16 8448
+#endif
+#ifndef MFP_LOWP_CAP32
+#define MFP_LOWP_CAP32 5632
+#endif
+#ifndef MFP_LOWP_STAGES
+#define MFP_LOWP_STAGES 2
+#endif
+#ifndef MFP_LOWP_TMA
+#define MFP_LOWP_TMA 1
+#endif
+
+template <int VT, bool D16>
+int lowp_tma_launch(const d::lowp_args<VT, D16> &A, uint32_t nnz, cudaStream_t s) {
+  constexpr uint32_t CAP = D16 ? MFP_LOWP_CAP16 : MFP_LOWP_CAP32;
+  constexpr uint32_t S = MFP_LOWP_STAGES;
+  static_assert(CAP % 8 == 0 && CAP >= 8, "stage capacity must be a multiple of 8 elements");
+  auto k = d::lowp_tma_kernel<VT, D16, CAP, S>;
+  const size_t dyn = d::lowp_pipe_bytes<D16, CAP, S>();
+  int st = ensure_dyn_smem((const void *)k, dyn, "lowp_tma_kernel");
+  if (st) return st;
+  uint32_t grid = 0;
+  if ((st = persistent_grid((const void *)k, (int)d::kLowpThreads, dyn, &grid))) return st;
+  grid = std::min(grid, ceil_div(A.n_rows, d::kLowpRows));
+  k<<<grid, d::kLowpThreads, dyn, s>>>(A, nnz);
+  return check_launch("lowp_tma_kernel launch");
+}
+
+int lowp_spmv(int vt, uint32_t rows, uint32_t nnz, const uint32_t *rp, const uint16_t *q, const float *scale,
+              const uint32_t *cols, const uint16_t *delta, const uint32_t *base, const float *x, float *y,
+              void *stream) {
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (rows == 0) return ok();
+  if (rows > 0xffffff00u) return fail(MFP_ERROR_TOO_LARGE, "too many rows");
+  if (!rp || !scale || !y || (nnz && (!q || !x || (!cols && !(delta && base)))))
+    return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  const bool d16 = cols == nullptr;
+  const bool vec = aligned16(q) && (d16 ? aligned16(delta) : aligned16(cols));
+  cudaStream_t s = as_stream(stream);
+  // TMA bulk copies need 16-byte-aligned sources: values, indices and row_ptr
+  if (MFP_LOWP_TMA && nnz && vec && aligned16(rp)) {
+    if (vt == MFP_BF16)
+      return d16 ? lowp_tma_launch<2, true>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s)
+                 : lowp_tma_launch<2, false>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s);
+    return d16 ? lowp_tma_launch<3, true>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s)
+               : lowp_tma_launch<3, false>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s);
+  }
+  const uint32_t grid = ceil_div(rows, d::kBlock);
+#define MFP_LOWP(VT, D16, VEC)                                                     \
+  {                                                                                \
+    d::lowp_args<VT, D16> A{rows, rp, q, scale, cols, delta, base, x, y};          \
+    d::lowp_kernel<VT, D16, VEC><<<grid, d::kBlock, 0, s>>>(A);                    \
+  }
+  if (vt == MFP_BF16) {
+    if (d16) {
+      if (vec) MFP_LOWP(2, true, true) else MFP_LOWP(2, true, false)
+    } else {
+      if (vec) MFP_LOWP(2, false, true) else MFP_LOWP(2, false, false)
+    }
+  } else {
+    if (d16) {
+      if (vec) MFP_LOWP(3, true, true) else MFP_LOWP(3, true, false)
+    } else {
+      if (vec) MFP_LOWP(3, false, true) else MFP_LOWP(3, false, false)
+    }
+  }
+#undef MFP_LOWP
+  return check_launch("lowp_kernel launch");
 }
 
 // Hybrid: the ELL kernel writes every row's ELL part, then the tile-based COO
@@ -629,6 +749,25 @@ int mfp_scoo_spmv_f64(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, 
                       double *y, void *s) {
   return scoo_spmv<double>(rows, slices, slice, v, ci, ri, sp, win, maxw, x, y, s);
 }
+int mfp_lowp_spmv(int vt, uint32_t rows, uint32_t, uint32_t nnz, const uint32_t *rp, const uint16_t *q,
+                  const float *scale, const uint32_t *cols, const uint16_t *delta, const uint32_t *base,
+                  const float *x, float *y, void *s) {
+  return lowp_spmv(vt, rows, nnz, rp, q, scale, cols, delta, base, x, y, s);
+}
+int mfp_lowp_error(int device, int clear, uint32_t *error) {
+  if (!error) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  int prev = 0;
+  CUDA_TRY(cudaGetDevice(&prev), "cudaGetDevice");
+  CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+  cudaError_t e = cudaMemcpyFromSymbol(error, d::g_lowp_error, sizeof(uint32_t));
+  if (e == cudaSuccess && clear) {
+    const uint32_t zero = 0;
+    e = cudaMemcpyToSymbol(d::g_lowp_error, &zero, sizeof(uint32_t));
+  }
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return cuda_fail(e, "lowp error word");
+  return ok();
+}
 int mfp_hybrid_workspace_bytes(uint32_t rows, uint32_t coo_nnz, size_t *bytes) {
   if (!bytes) return fail(MFP_ERROR_INVALID_VALUE, "null output");
   *bytes = coo_ws_bytes(coo_nnz);
@@ -672,6 +811,10 @@ struct mfp_matrix {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   void *dx = nullptr, *dy = nullptr;  // staging for the host-buffer call
+  int lowp_vt = 0;                    // reduced-precision CSR: MFP_BF16 / MFP_F16
+  float *scale = nullptr;
+  uint16_t *delta = nullptr;          // 16-bit column deltas (else cols_a)
+  uint32_t *base = nullptr;
 };
 
 namespace {
@@ -935,16 +1078,58 @@ int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t widt
   return finish_matrix(m, out);
 }
 
+int mfp_matrix_create_lowp(int vt, int index16, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
+                           const uint32_t *ci, const double *v, mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (nnz && (!ci || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  int st = check_row_ptr(rows, nnz, rp);
+  if (st) return st;
+  if ((st = check_columns(ci, nnz, cols))) return st;
+  std::vector<uint16_t> q(nnz), dl;
+  std::vector<float> sc(rows);
+  std::vector<uint32_t> bs;
+  if ((st = mfp_lowp_quantize(vt, rows, rp, v, q.data(), sc.data()))) return st;
+  if (index16) {
+    dl.resize(nnz);
+    bs.resize(((uint64_t)nnz + MFP_LOWP_DELTA_CHUNK - 1) / MFP_LOWP_DELTA_CHUNK);
+    if ((st = mfp_lowp_deltas(nnz, ci, dl.data(), bs.data()))) return st;
+  }
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_CSR_LOWP;
+  m->value_type = MFP_F32;  // x and y
+  m->lowp_vt = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  m->format_bytes = (uint64_t)nnz * (index16 ? 4 : 6) + (uint64_t)bs.size() * 4 + (uint64_t)rows * 4 +
+                    ((uint64_t)rows + 1) * 4 + (uint64_t)cols * 4 + (uint64_t)rows * 4;
+  if ((st = track_upload(m, &m->rows_a, rp, (size_t)rows + 1)) || (st = track_upload(m, &m->scale, sc.data(), sc.size())) ||
+      (st = track_upload_bytes(m, &m->vals, q.data(), q.size() * 2)) ||
+      (index16 ? ((st = track_upload(m, &m->delta, dl.data(), dl.size())) ||
+                  (st = track_upload(m, &m->base, bs.data(), bs.size())))
+               : (st = track_upload(m, &m->cols_a, ci, nnz)))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  return finish_matrix(m, out);
+}
+
 int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
   if (!m || !out) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   const size_t vs = value_size(m->value_type);
   out->format = m->format;
-  out->value_type = m->value_type;
+  out->value_type = m->format == MFP_FORMAT_CSR_LOWP ? m->lowp_vt : m->value_type;
   out->rows = m->rows;
   out->cols = m->cols;
   out->nnz = m->nnz;
   out->format_bytes = m->format_bytes;
   out->algorithmic_bytes = m->nnz * (vs + 4) + ((uint64_t)m->rows + 1) * 4 + (uint64_t)m->cols * vs + (uint64_t)m->rows * vs;
+  if (m->format == MFP_FORMAT_CSR_LOWP)  // 16-bit values, uint32 column ids, row scales
+    out->algorithmic_bytes = m->nnz * 6 + (uint64_t)m->rows * 4 + ((uint64_t)m->rows + 1) * 4 +
+                             (uint64_t)m->cols * 4 + (uint64_t)m->rows * 4;
   out->device_bytes = m->device_bytes;
   out->kernel_launches = (m->format == MFP_FORMAT_HYBRID && m->coo_nnz) ? 2 : 1;
   return ok();
@@ -983,6 +1168,9 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                  : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
                                    (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
                                    m->ws_bytes, stream);
+    case MFP_FORMAT_CSR_LOWP:
+      return lowp_spmv(m->lowp_vt, m->rows, (uint32_t)m->nnz, m->rows_a, (const uint16_t *)m->vals, m->scale,
+                       m->delta ? nullptr : m->cols_a, m->delta, m->base, (const float *)x, (float *)y, stream);
     default:
       return fail(MFP_ERROR_INVALID_VALUE, "unknown format %d", m->format);
   }

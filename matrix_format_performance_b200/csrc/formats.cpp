@@ -360,6 +360,55 @@ int mfp_compare_results_f64(uint32_t n, const double *a, const double *b, double
   return compare<double>(n, a, b, e, fb);
 }
 
+// ---- reduced-precision CSR (engine extension) ------------------------------
+static uint16_t to_bf16_rne(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+static uint16_t to_fp16(float f) {
+  const _Float16 h = (_Float16)f;  // round-to-nearest-even
+  uint16_t u;
+  std::memcpy(&u, &h, 2);
+  return u;
+}
+
+int mfp_lowp_quantize(int vt, uint32_t rows, const uint32_t *rp, const double *v, uint16_t *q, float *scale) {
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (!rp || !scale) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const uint32_t nnz = rp[rows];
+  if (nnz && (!v || !q)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  for (uint32_t r = 0; r < rows; ++r) {
+    double mx = 0.0;
+    for (uint32_t e = rp[r]; e < rp[r + 1]; ++e) mx = std::max(mx, std::fabs(v[e]));
+    const float s = mx > 0.0 ? (float)mx : 1.0f;
+    scale[r] = s;
+    for (uint32_t e = rp[r]; e < rp[r + 1]; ++e) {
+      const float f = (float)(v[e] / (double)s);
+      q[e] = vt == MFP_BF16 ? to_bf16_rne(f) : to_fp16(f);
+    }
+  }
+  return ok();
+}
+
+int mfp_lowp_deltas(uint32_t nnz, const uint32_t *c, uint16_t *delta, uint32_t *base) {
+  if (nnz && (!c || !delta || !base)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const uint32_t chunks = (uint32_t)(((uint64_t)nnz + MFP_LOWP_DELTA_CHUNK - 1) / MFP_LOWP_DELTA_CHUNK);
+  for (uint32_t k = 0; k < chunks; ++k) {
+    const uint32_t b = k * MFP_LOWP_DELTA_CHUNK, e = (uint32_t)std::min<uint64_t>(nnz, (uint64_t)b + MFP_LOWP_DELTA_CHUNK);
+    uint32_t lo = UINT32_MAX, hi = 0;
+    for (uint32_t i = b; i < e; ++i) {
+      lo = std::min(lo, c[i]);
+      hi = std::max(hi, c[i]);
+    }
+    if (hi - lo > 65535u)
+      return fail(MFP_ERROR_NOT_SUPPORTED, "16-bit deltas: columns of chunk %u span %u > 65535", k, hi - lo);
+    base[k] = lo;
+    for (uint32_t i = b; i < e; ++i) delta[i] = (uint16_t)(c[i] - lo);
+  }
+  return ok();
+}
+
 int mfp_scoo_x_windows(uint32_t nnz, const uint32_t *ci, const uint32_t *sp, uint32_t slices,
                        uint32_t *win) {
   if (!sp || !win || (nnz && !ci)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");

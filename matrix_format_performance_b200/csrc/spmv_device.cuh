@@ -185,112 +185,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
   return s_warp[warp] + inc - v;
 }
 
-// ---- staging ---------------------------------------------------------------
-// Writes p[e] = vals[e] * x[cols[e]] for e in [a, b) to dst[e - (a & ~3)].
-// The matrix arrays are read with 16-byte loads on 4-element groups (VEC) and
-// the products are stored as whole groups, so shared-memory stores are 16- or
-// 32-byte wide and conflict-free.  dst must hold b - (a & ~3) elements.
-template <typename T, int BLOCK, bool VEC>
-__device__ __forceinline__ void stage_products(const T *__restrict__ vals,
-                                               const uint32_t *__restrict__ cols,
-                                               const T *__restrict__ x, uint32_t a, uint32_t b,
-                                               T *__restrict__ dst, uint64_t pol) {
-  const uint32_t base = a & ~3u;
-  if (VEC) {
-    const uint32_t a4 = (a + 3u) & ~3u;
-    const uint32_t b4 = b & ~3u;
-    if (a4 < b4) {
-      // head [a, a4), body [a4, b4), tail [b4, b)
-      if (threadIdx.x < a4 - a) {
-        const uint32_t e = a + threadIdx.x;
-        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-      }
-      if (threadIdx.x < b - b4) {
-        const uint32_t e = b4 + threadIdx.x;
-        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-      }
-      const uint32_t ng = (b4 - a4) >> 2;
-      uint32_t g = threadIdx.x;
-      for (; g + BLOCK < ng; g += 2 * BLOCK) {
-        const uint32_t e0 = a4 + 4u * g, e1 = e0 + 4u * BLOCK;
-        T v0[4], v1[4];
-        uint32_t c0[4], c1[4];
-        ld_stream4(vals + e0, v0, pol);
-        ld_stream4(cols + e0, c0, pol);
-        ld_stream4(vals + e1, v1, pol);
-        ld_stream4(cols + e1, c1, pol);
-        T p0[4], p1[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) p0[k] = mul_rn(v0[k], ld_x(x + c0[k]));
-#pragma unroll
-        for (int k = 0; k < 4; ++k) p1[k] = mul_rn(v1[k], ld_x(x + c1[k]));
-#pragma unroll
-        for (int k = 0; k < 4; ++k) dst[e0 - base + k] = p0[k];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) dst[e1 - base + k] = p1[k];
-      }
-      if (g < ng) {
-        const uint32_t e0 = a4 + 4u * g;
-        T v0[4];
-        uint32_t c0[4];
-        ld_stream4(vals + e0, v0, pol);
-        ld_stream4(cols + e0, c0, pol);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) dst[e0 - base + k] = mul_rn(v0[k], ld_x(x + c0[k]));
-      }
-      return;
-    }
-  }
-  for (uint32_t e = a + threadIdx.x; e < b; e += BLOCK)
-    dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-}
-
-// Same, also staging the row id of every element (COO-like layouts).
-template <typename T, int BLOCK, bool VEC>
-__device__ __forceinline__ void stage_products_rows(const T *__restrict__ vals,
-                                                    const uint32_t *__restrict__ cols,
-                                                    const uint32_t *__restrict__ rows,
-                                                    const T *__restrict__ x, uint32_t a, uint32_t b,
-                                                    T *__restrict__ dst, uint32_t *__restrict__ dst_rows,
-                                                    uint64_t pol) {
-  const uint32_t base = a & ~3u;
-  if (VEC) {
-    const uint32_t a4 = (a + 3u) & ~3u;
-    const uint32_t b4 = b & ~3u;
-    if (a4 < b4) {
-      if (threadIdx.x < a4 - a) {
-        const uint32_t e = a + threadIdx.x;
-        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-        dst_rows[e - base] = ld_stream1(rows + e, pol);
-      }
-      if (threadIdx.x < b - b4) {
-        const uint32_t e = b4 + threadIdx.x;
-        dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-        dst_rows[e - base] = ld_stream1(rows + e, pol);
-      }
-      const uint32_t ng = (b4 - a4) >> 2;
-      for (uint32_t g = threadIdx.x; g < ng; g += BLOCK) {
-        const uint32_t e0 = a4 + 4u * g;
-        T v0[4];
-        uint32_t c0[4], r0[4];
-        ld_stream4(vals + e0, v0, pol);
-        ld_stream4(cols + e0, c0, pol);
-        ld_stream4(rows + e0, r0, pol);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          dst[e0 - base + k] = mul_rn(v0[k], ld_x(x + c0[k]));
-          dst_rows[e0 - base + k] = r0[k];
-        }
-      }
-      return;
-    }
-  }
-  for (uint32_t e = a + threadIdx.x; e < b; e += BLOCK) {
-    dst[e - base] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-    dst_rows[e - base] = ld_stream1(rows + e, pol);
-  }
-}
-
 // Bounded spin on a flag written by an earlier CTA of the same launch.
 // Returns false (and the caller records an error) if the limit is reached.
 __device__ __forceinline__ bool wait_flag(const uint32_t *flag, uint32_t limit) {
@@ -336,6 +230,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "r"(smem_addr(bar)), "r"(parity)
       : "memory");
   return done != 0;
+}
+// Plain arrival (no transaction bytes); release semantics at CTA scope.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 // Bounded wait: false if the phase did not complete within `limit` polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {

@@ -17,13 +17,15 @@ from ._capi import call
 from .formats import (coo_matrix_class, csr_matrix_class, ell_matrix_class, hybrid_matrix_class, ptr,
                       scoo_matrix_class)
 
-CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID = range(7)
+CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID, CSR_LOWP = range(8)
+BF16, F16 = 2, 3
 FORMAT_NAMES = {"csr": CSR_SCALAR, "csr_vector": CSR_VECTOR, "csr_adaptive": CSR_ADAPTIVE, "ell": ELL,
                 "coo": COO, "scoo": SCOO, "hybrid": HYBRID}
 # JSON labels of the reference (gpu_matrix_multiplier.cu:129, :443, :546, :712, :1092;
 # csr_adaptive_spmv.cu:320; scoo_spmv.cu:221)
 LABELS = {CSR_SCALAR: "GPU CSR", CSR_VECTOR: "GPU CSR (vector)", CSR_ADAPTIVE: "GPU CSR-Adaptive", ELL: "GPU ELL",
-          COO: "GPU COO", SCOO: "GPU SCOO", HYBRID: "GPU Hybrid (atomic)"}
+          COO: "GPU COO", SCOO: "GPU SCOO", HYBRID: "GPU Hybrid (atomic)",
+          CSR_LOWP: "GPU CSR (16-bit values)"}
 _VT = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}
 
 
@@ -94,6 +96,17 @@ class DeviceMatrix:
         call("mfp_matrix_create_hybrid", _VT[e.dtype], e.rows, e.cols, e.elements_in_rows, ptr(e.columns),
              ptr(e.data), c.elements_count, ptr(c.rows_), ptr(c.cols_), ptr(c.data), C.byref(h))
         return cls(h, HYBRID, e.dtype)
+
+    @classmethod
+    def from_csr_lowp(cls, m: csr_matrix_class, value_type: int = BF16, index16: bool = False) -> "DeviceMatrix":
+        """16-bit values (BF16/FP16) with per-row FP32 scales; x and y float32."""
+        v = np.ascontiguousarray(m.data, np.float64)
+        h = C.c_void_p()
+        call("mfp_matrix_create_lowp", value_type, int(index16), m.rows, m.cols, m.nnz, ptr(m.row_ptr),
+             ptr(m.columns), ptr(v), C.byref(h))
+        dm = cls(h, CSR_LOWP, np.float32)
+        dm.label = f"GPU CSR ({'BF16' if value_type == BF16 else 'FP16'}{', 16-bit deltas' if index16 else ''})"
+        return dm
 
     @classmethod
     def build(cls, m: csr_matrix_class, fmt: int, *, sm_count: int = 148, shared_mem: int = 49152,

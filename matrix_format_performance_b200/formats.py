@@ -227,3 +227,22 @@ def compare_results(a: np.ndarray, b: np.ndarray) -> tuple[float, int | None]:
     aa, bb = np.ascontiguousarray(a), np.ascontiguousarray(b)  # alive across the call
     call(f"mfp_compare_results_{_SFX[a.dtype]}", a.size, ptr(aa), ptr(bb), C.byref(err), C.byref(bad))
     return err.value, (None if bad.value == 0xFFFFFFFF else int(bad.value))
+
+
+def lowp_quantize(m: csr_matrix_class, value_type: int):
+    """16-bit value bit patterns and per-row scales (mfp_lowp_quantize)."""
+    v = np.ascontiguousarray(m.data, np.float64)
+    q = np.empty(m.nnz, np.uint16)
+    sc = np.empty(m.rows, np.float32)
+    call("mfp_lowp_quantize", value_type, m.rows, ptr(m.row_ptr), ptr(v), ptr(q), ptr(sc))
+    return q, sc
+
+
+def lowp_dequantize(q: np.ndarray, scale: np.ndarray, row_ptr: np.ndarray, value_type: int) -> np.ndarray:
+    """Exact float64 values scale_i * float(q_ij) of a reduced-precision CSR."""
+    if value_type == 2:
+        f = (q.astype(np.uint32) << 16).view(np.float32)
+    else:
+        f = q.view(np.float16).astype(np.float32)
+    rows = np.repeat(np.arange(row_ptr.size - 1), np.diff(row_ptr.astype(np.int64)))
+    return f.astype(np.float64) * scale.astype(np.float64)[rows]
