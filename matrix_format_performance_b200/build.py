@@ -87,6 +87,29 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, d
     return lib
 
 
+HOST = PKG / "host"
+DRIVER = LIBDIR / "mfp_driver"
+HOST_HEADERS = ["matrix_market_reader.h", "matrix_converter.h", "scoo_matrix_class.h", "measurement_class.h",
+                "resizable_gpu_memory.h", "gpu_matrix_multiplier.h", "cpu_matrix_multiplier.h"]
+
+
+def host_compile(src: Path, out: Path, extra: list[str] | None = None) -> Path:
+    """Compiles a C++ program against the host layer (host/*.h) and libmfp_spmv.so."""
+    out.parent.mkdir(parents=True, exist_ok=True)
+    deps = [src, LIB] + [HOST / h for h in HOST_HEADERS] + [ROOT / "include" / "mfp_spmv.h"]
+    if _stale(out, deps):
+        _run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Wno-unused-parameter", f"-I{ROOT / 'include'}",
+              f"-I{HOST}", f"-I{CUDA_HOME / 'include'}", str(src), "-o", str(out), f"-L{LIBDIR}", "-lmfp_spmv",
+              f"-L{CUDA_HOME / 'lib64'}", "-lcudart_static", "-ldl", "-lrt", "-lpthread",
+              f"-Wl,-rpath,{LIBDIR}"] + (extra or []))
+    return out
+
+
+def build_driver() -> Path:
+    """The main.cpp-style benchmark driver (host/main.cpp) -> lib/mfp_driver."""
+    return host_compile(HOST / "main.cpp", DRIVER)
+
+
 def clean() -> None:
     shutil.rmtree(BUILD, ignore_errors=True)
     if LIB.exists():
@@ -103,6 +126,7 @@ def main() -> None:
         clean()
         return
     build(force=a.force, jobs=a.jobs, verbose=True)
+    print(f"built {build_driver()}")
 
 
 if __name__ == "__main__":
