@@ -287,6 +287,49 @@ int mfp_lowp_spmv(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz, co
  * resets it.  Synchronous.  Engine extension, no counterpart in the reference. */
 int mfp_lowp_error(int device, int clear, uint32_t *error);
 
+/* ---- Batched SpMV (engine extension, no counterpart in the reference) ------
+ * Many CSR matrices of uneven sizes as one block-diagonal CSR: matrix k's rows
+ * follow matrix k-1's, its column ids are shifted into its own slice of one
+ * concatenated x, and its y is a slice of one concatenated y
+ * (mfp_batch_offsets).  One launch covers every matrix.  The plan (algorithm,
+ * lanes, thresholds, kernel) is the default CSR scalar plan until
+ * mfp_batch_set_config or mfp_batch_autotune picks another;
+ * mfp_batch_graph_launch captures the launch into a CUDA graph once per
+ * (x, y) pair and replays it. */
+typedef struct mfp_batch mfp_batch;
+typedef struct mfp_batch_config {
+  int algo;              /* 0 CSR scalar, 1 CSR vector, 2 CSR-Adaptive */
+  mfp_csr_config csr;    /* lanes, thresholds, kernel (0 fields = defaults) */
+} mfp_batch_config;
+typedef struct mfp_batch_info {
+  uint32_t matrices, rows, cols, nnz; /* totals of the concatenation */
+  uint64_t algorithmic_bytes;         /* sum over the matrices of nnz*(v+4)+(rows+1)*4+cols*v+rows*v */
+  uint64_t device_bytes;
+  mfp_batch_config config;            /* the plan in use */
+  uint32_t kernel_launches;           /* launches per mfp_batch_spmv */
+} mfp_batch_info;
+/* Host CSR arrays per matrix: rows[k], cols[k], row_ptr[k] (rows[k]+1
+ * entries, nnz = row_ptr[k][rows[k]]), columns[k], values[k] (float or
+ * double).  Totals must fit 32-bit indices. */
+int mfp_batch_create(int value_type, uint32_t matrices, const uint32_t *rows, const uint32_t *cols,
+                     const uint32_t *const *row_ptr, const uint32_t *const *columns,
+                     const void *const *values, mfp_batch **out);
+int mfp_batch_destroy(mfp_batch *batch);
+/* x_offsets / y_offsets receive matrices+1 entries (element offsets). */
+int mfp_batch_offsets(const mfp_batch *batch, uint64_t *x_offsets, uint64_t *y_offsets);
+int mfp_batch_get_info(const mfp_batch *batch, mfp_batch_info *out);
+int mfp_batch_set_config(mfp_batch *batch, const mfp_batch_config *config);
+/* Times every candidate plan (reps launches each, median of CUDA-event times
+ * on `stream`) on the given x, y and keeps the fastest; *chosen and
+ * *best_seconds (either may be NULL) receive it.  Synchronous. */
+int mfp_batch_autotune(mfp_batch *batch, const void *x, void *y, uint32_t reps, void *stream,
+                       mfp_batch_config *chosen, double *best_seconds);
+int mfp_batch_spmv(const mfp_batch *batch, const void *x, void *y, void *stream);
+/* Replays a CUDA graph of mfp_batch_spmv(x, y); the first call for an (x, y)
+ * pair captures it (on an internal stream), so make that call outside any
+ * stream capture of the caller's. */
+int mfp_batch_graph_launch(mfp_batch *batch, const void *x, void *y, void *stream);
+
 /* fill_vector — gpu_matrix_multiplier.cu:45-52. */
 int mfp_fill_f32(uint64_t n, float *vec, float value, void *stream);
 int mfp_fill_f64(uint64_t n, double *vec, double value, void *stream);

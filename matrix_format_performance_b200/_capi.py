@@ -157,3 +157,24 @@ def check(status: int) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(load(), name)(*args))
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("algo", i32), ("csr", CsrConfig)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("matrices", u32), ("rows", u32), ("cols", u32), ("nnz", u32), ("algorithmic_bytes", u64),
+                ("device_bytes", u64), ("config", BatchConfig), ("kernel_launches", u32)]
+
+
+_PROTOS.update({
+    "mfp_batch_create": [i32, u32, vp, vp, vp, vp, vp, C.POINTER(vp)],
+    "mfp_batch_destroy": [vp],
+    "mfp_batch_offsets": [vp, vp, vp],
+    "mfp_batch_get_info": [vp, C.POINTER(BatchInfo)],
+    "mfp_batch_set_config": [vp, C.POINTER(BatchConfig)],
+    "mfp_batch_autotune": [vp, vp, vp, u32, vp, C.POINTER(BatchConfig), C.POINTER(f64)],
+    "mfp_batch_spmv": [vp, vp, vp, vp],
+    "mfp_batch_graph_launch": [vp, vp, vp, vp],
+})

@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -1235,6 +1237,269 @@ int mfp_matrix_time(const mfp_matrix *m, const void *x, void *y, uint32_t reps, 
   std::sort(t.begin(), t.end());
   if (mean_s) *mean_s = sum / reps;
   if (median_s) *median_s = t[t.size() / 2];
+  return ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched SpMV: many matrices as one block-diagonal CSR (engine extension)
+// ---------------------------------------------------------------------------
+struct mfp_batch {
+  int device = 0, vt = 0;
+  uint32_t n = 0, rows = 0, cols = 0, nnz = 0;
+  std::vector<uint64_t> x_off, y_off;
+  std::vector<uint32_t> host_rp;  // concatenated row_ptr (for re-planning)
+  uint64_t algorithmic_bytes = 0;
+  void *vals = nullptr;
+  uint32_t *cols_a = nullptr, *rp = nullptr;
+  size_t array_bytes = 0;
+  mfp_csr_plan *plan = nullptr;
+  mfp_batch_config cfg{};
+  // captured graph of one launch for (gx, gy)
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *gx = nullptr;
+  void *gy = nullptr;
+};
+
+namespace {
+void batch_drop_graph(mfp_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+  b->gx = nullptr;
+  b->gy = nullptr;
+}
+int batch_plan(mfp_batch *b, const mfp_batch_config &c, mfp_csr_plan **out) {
+  if (c.algo < 0 || c.algo > 2) return fail(MFP_ERROR_INVALID_VALUE, "batch algo must be 0, 1 or 2");
+  return mfp_csr_plan_create(b->rows, b->cols, b->nnz, b->host_rp.data(), c.algo, &c.csr, out);
+}
+int batch_launch(const mfp_batch *b, const mfp_csr_plan *plan, const void *x, void *y, void *stream) {
+  return b->vt == MFP_F64 ? csr_spmv<double>(plan, (const double *)b->vals, b->cols_a, b->rp, (const double *)x,
+                                             (double *)y, stream)
+                          : csr_spmv<float>(plan, (const float *)b->vals, b->cols_a, b->rp, (const float *)x,
+                                            (float *)y, stream);
+}
+}  // namespace
+
+extern "C" {
+
+int mfp_batch_create(int vt, uint32_t n, const uint32_t *rows, const uint32_t *cols, const uint32_t *const *row_ptr,
+                     const uint32_t *const *columns, const void *const *values, mfp_batch **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
+  if (n && (!rows || !cols || !row_ptr || !columns || !values)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const size_t vs = value_size(vt);
+  auto b = std::make_unique<mfp_batch>();
+  cudaGetDevice(&b->device);
+  b->vt = vt;
+  b->n = n;
+  b->x_off.assign((size_t)n + 1, 0);
+  b->y_off.assign((size_t)n + 1, 0);
+  uint64_t R = 0, Cn = 0, Z = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    if (!row_ptr[k]) return fail(MFP_ERROR_INVALID_VALUE, "null row_ptr of matrix %u", k);
+    const uint32_t nz = row_ptr[k][rows[k]];
+    int st = check_row_ptr(rows[k], nz, row_ptr[k]);
+    if (!st && nz && (!columns[k] || !values[k])) st = fail(MFP_ERROR_INVALID_VALUE, "null arrays");
+    if (!st) st = check_columns(columns[k], nz, cols[k]);
+    if (st) {
+      const std::string msg = mfp_last_error();
+      return fail(st, "matrix %u: %s", k, msg.c_str());
+    }
+    b->x_off[k] = Cn;
+    b->y_off[k] = R;
+    R += rows[k];
+    Cn += cols[k];
+    Z += nz;
+    b->algorithmic_bytes += (uint64_t)nz * (vs + 4) + ((uint64_t)rows[k] + 1) * 4 + (uint64_t)cols[k] * vs +
+                            (uint64_t)rows[k] * vs;
+  }
+  b->x_off[n] = Cn;
+  b->y_off[n] = R;
+  if (R >= UINT32_MAX || Cn >= UINT32_MAX || Z >= UINT32_MAX)
+    return fail(MFP_ERROR_TOO_LARGE, "batch totals exceed 32-bit indexing (rows %llu, cols %llu, nnz %llu)",
+                (unsigned long long)R, (unsigned long long)Cn, (unsigned long long)Z);
+  b->rows = (uint32_t)R;
+  b->cols = (uint32_t)Cn;
+  b->nnz = (uint32_t)Z;
+  b->host_rp.resize((size_t)R + 1);
+  std::vector<uint32_t> hc(Z);
+  std::vector<unsigned char> hv(Z * vs);
+  uint64_t r0 = 0, z0 = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t nz = row_ptr[k][rows[k]];
+    for (uint32_t r = 0; r < rows[k]; ++r) b->host_rp[r0 + r] = (uint32_t)(z0 + row_ptr[k][r]);
+    const uint32_t xo = (uint32_t)b->x_off[k];
+    for (uint32_t e = 0; e < nz; ++e) hc[z0 + e] = columns[k][e] + xo;
+    if (nz) std::memcpy(hv.data() + z0 * vs, values[k], (size_t)nz * vs);
+    r0 += rows[k];
+    z0 += nz;
+  }
+  b->host_rp[R] = (uint32_t)Z;
+  unsigned char *dv = nullptr;
+  int st;
+  if ((st = dmalloc(&dv, hv.size(), &b->array_bytes)) || (st = dmalloc(&b->cols_a, hc.size(), &b->array_bytes)) ||
+      (st = dmalloc(&b->rp, b->host_rp.size(), &b->array_bytes))) {
+    cudaFree(dv);
+    mfp_batch_destroy(b.release());
+    return st;
+  }
+  b->vals = dv;
+  if ((!hv.empty() && cudaMemcpy(dv, hv.data(), hv.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (!hc.empty() && cudaMemcpy(b->cols_a, hc.data(), hc.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(b->rp, b->host_rp.data(), b->host_rp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    mfp_batch_destroy(b.release());
+    return fail(MFP_ERROR_CUDA, "batch upload failed");
+  }
+  b->cfg = mfp_batch_config{};
+  if ((st = batch_plan(b.get(), b->cfg, &b->plan))) {
+    mfp_batch_destroy(b.release());
+    return st;
+  }
+  *out = b.release();
+  return ok();
+}
+
+int mfp_batch_destroy(mfp_batch *b) {
+  if (!b) return ok();
+  batch_drop_graph(b);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  mfp_csr_plan_destroy(b->plan);
+  cudaFree(b->vals);
+  cudaFree(b->cols_a);
+  cudaFree(b->rp);
+  delete b;
+  return ok();
+}
+
+int mfp_batch_offsets(const mfp_batch *b, uint64_t *xo, uint64_t *yo) {
+  if (!b) return fail(MFP_ERROR_INVALID_VALUE, "null batch");
+  if (xo) std::copy(b->x_off.begin(), b->x_off.end(), xo);
+  if (yo) std::copy(b->y_off.begin(), b->y_off.end(), yo);
+  return ok();
+}
+
+int mfp_batch_get_info(const mfp_batch *b, mfp_batch_info *out) {
+  if (!b || !out) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  out->matrices = b->n;
+  out->rows = b->rows;
+  out->cols = b->cols;
+  out->nnz = b->nnz;
+  out->algorithmic_bytes = b->algorithmic_bytes;
+  out->device_bytes = b->array_bytes + (b->plan ? b->plan->device_bytes : 0);
+  out->config = b->cfg;
+  out->kernel_launches = b->nnz ? 1 : (b->rows ? 1 : 0);
+  return ok();
+}
+
+int mfp_batch_set_config(mfp_batch *b, const mfp_batch_config *c) {
+  if (!b || !c) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  mfp_csr_plan *p = nullptr;
+  int st = batch_plan(b, *c, &p);
+  if (st) return st;
+  batch_drop_graph(b);
+  mfp_csr_plan_destroy(b->plan);
+  b->plan = p;
+  b->cfg = *c;
+  return ok();
+}
+
+int mfp_batch_spmv(const mfp_batch *b, const void *x, void *y, void *stream) {
+  if (!b) return fail(MFP_ERROR_INVALID_VALUE, "null batch");
+  return batch_launch(b, b->plan, x, y, stream);
+}
+
+int mfp_batch_autotune(mfp_batch *b, const void *x, void *y, uint32_t reps, void *stream, mfp_batch_config *chosen,
+                       double *best_seconds) {
+  if (!b || reps == 0) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
+  // the candidate plans: CSR scalar with several warp-assist and long-row
+  // thresholds, the streaming (persistent) kernel, CSR vector lane counts and
+  // CSR-Adaptive bin sizes
+  std::vector<mfp_batch_config> cand;
+  auto add = [&](int algo, uint32_t lanes, uint32_t bin, uint32_t assist, uint32_t longt, uint32_t kernel) {
+    mfp_batch_config c{};
+    c.algo = algo;
+    c.csr.vector_lanes = lanes;
+    c.csr.bin_nnz = bin;
+    c.csr.assist_threshold = assist;
+    c.csr.long_row_threshold = longt;
+    c.csr.kernel = kernel;
+    cand.push_back(c);
+  };
+  for (uint32_t assist : {32u, 64u, 256u})
+    for (uint32_t longt : {2048u, 4096u, 16384u}) add(0, 0, 0, assist, longt, 1);
+  add(0, 0, 0, 0, 0, 2);
+  add(0, 0, 0, 0, 0, 3);
+  for (uint32_t lanes : {0u, 4u, 8u, 32u}) add(1, lanes, 0, 0, 0, 1);
+  for (uint32_t bin : {0u, 1020u, 508u}) add(2, 0, bin, 0, 0, 1);
+  cudaStream_t s = as_stream(stream);
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0), "cudaEventCreate");
+  CUDA_TRY(cudaEventCreate(&e1), "cudaEventCreate");
+  double best = 1e300;
+  int best_i = -1, st = MFP_SUCCESS;
+  for (size_t i = 0; i < cand.size() && !st; ++i) {
+    mfp_csr_plan *p = nullptr;
+    if (batch_plan(b, cand[i], &p)) continue;  // a configuration the matrix does not admit
+    std::vector<double> t;
+    st = batch_launch(b, p, x, y, stream);  // warm-up
+    for (uint32_t r = 0; r < reps && !st; ++r) {
+      cudaEventRecord(e0, s);
+      st = batch_launch(b, p, x, y, stream);
+      cudaEventRecord(e1, s);
+      if (!st) {
+        const cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaEventSynchronize");
+      }
+      float ms = 0;
+      if (!st) cudaEventElapsedTime(&ms, e0, e1);
+      t.push_back(ms * 1e-3);
+    }
+    mfp_csr_plan_destroy(p);
+    if (st) break;
+    std::sort(t.begin(), t.end());
+    const double med = t[t.size() / 2];
+    if (med < best) {
+      best = med;
+      best_i = (int)i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  if (best_i < 0) return fail(MFP_ERROR_NOT_SUPPORTED, "no candidate plan could be built");
+  if ((st = mfp_batch_set_config(b, &cand[best_i]))) return st;
+  if (chosen) *chosen = cand[best_i];
+  if (best_seconds) *best_seconds = best;
+  return ok();
+}
+
+int mfp_batch_graph_launch(mfp_batch *b, const void *x, void *y, void *stream) {
+  if (!b) return fail(MFP_ERROR_INVALID_VALUE, "null batch");
+  if (!b->exec || b->gx != x || b->gy != y) {
+    batch_drop_graph(b);
+    if (!b->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    const int st = batch_launch(b, b->plan, x, y, b->cap_stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    if (st) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+      b->exec = nullptr;
+      return cuda_fail(e2, "cudaGraphInstantiate");
+    }
+    b->gx = x;
+    b->gy = y;
+  }
+  CUDA_TRY(cudaGraphLaunch(b->exec, as_stream(stream)), "cudaGraphLaunch");
   return ok();
 }
 
