@@ -330,6 +330,38 @@ int mfp_batch_spmv(const mfp_batch *batch, const void *x, void *y, void *stream)
  * stream capture of the caller's. */
 int mfp_batch_graph_launch(mfp_batch *batch, const void *x, void *y, void *stream);
 
+/* ---- Format selector (engine extension, no counterpart in the reference) --
+ * Features of a CSR pattern (host):
+ *   0 log10(rows)          1 log10(cols)            2 log10(nnz + 1)
+ *   3 log2(1 + mean len)   4 log2(1 + std of len)   5 log2(1 + max len)
+ *   6 Gini of row lengths  7 max |i - j| / max(rows, cols)   (bandwidth)
+ *   8 share of nonzeros with |i - j| <= 64           9 diagonal nonzeros / min(rows, cols)
+ *  10 share of empty rows  11 share of nonzeros in rows longer than 4096 */
+#define MFP_SELECTOR_FEATURES 12u
+int mfp_selector_features(uint32_t rows, uint32_t cols, const uint32_t *row_ptr, const uint32_t *columns,
+                          float *features);
+
+/* The selector's MLP 12 -> 64 -> 64 -> 28 (ReLU hidden layers), FP32, device
+ * arrays, enqueued on `stream`.  params: W1[12][64] b1[64] W2[64][64] b2[64]
+ * W3[64][28] b3[28] (mfp_mlp_param_count() floats).  All sums run in a fixed
+ * order, so results are reproducible. */
+#define MFP_MLP_IN 12u
+#define MFP_MLP_HIDDEN 64u
+#define MFP_MLP_OUT 28u
+uint32_t mfp_mlp_param_count(void);
+/* h1[batch][64], h2[batch][64], y[batch][28]. */
+int mfp_mlp_forward(const float *params, const float *x, uint32_t batch, float *h1, float *h2, float *y,
+                    void *stream);
+/* Masked mean-squared error of y against target (mask 0/1, [batch][28]):
+ * *loss (device) = sum mask (y - target)^2 / sum mask; grads (param count
+ * floats) its gradient; work holds batch * (28 + 64 + 64) floats. */
+int mfp_mlp_backward(const float *params, const float *x, const float *h1, const float *h2, const float *y,
+                     const float *target, const float *mask, uint32_t batch, float *grads, float *loss,
+                     float *work, void *stream);
+/* One Adam step (bias-corrected; step counts from 1). */
+int mfp_mlp_adam(float *params, const float *grads, float *m, float *v, uint32_t n, float lr, float beta1,
+                 float beta2, float eps, uint32_t step, void *stream);
+
 /* fill_vector — gpu_matrix_multiplier.cu:45-52. */
 int mfp_fill_f32(uint64_t n, float *vec, float value, void *stream);
 int mfp_fill_f64(uint64_t n, double *vec, double value, void *stream);

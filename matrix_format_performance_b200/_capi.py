@@ -178,3 +178,11 @@ _PROTOS.update({
     "mfp_batch_spmv": [vp, vp, vp, vp],
     "mfp_batch_graph_launch": [vp, vp, vp, vp],
 })
+_PROTOS.update({
+    "mfp_selector_features": [u32, u32, vp, vp, vp],
+    "mfp_mlp_param_count": [],
+    "mfp_mlp_forward": [vp, vp, u32, vp, vp, vp, vp],
+    "mfp_mlp_backward": [vp, vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp],
+    "mfp_mlp_adam": [vp, vp, vp, vp, u32, C.c_float, C.c_float, C.c_float, C.c_float, u32, vp],
+})
+_RESTYPES["mfp_mlp_param_count"] = u32

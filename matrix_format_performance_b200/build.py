@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["capi.cu"]
 CPP_SOURCES = ["util.cpp", "formats.cpp", "synth.cpp"]
-HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "spmv_stream.cuh", "spmv_lowp.cuh", "host_common.h"]
+HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "spmv_stream.cuh", "spmv_lowp.cuh", "mlp.cuh", "host_common.h"]
 
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3",
                      "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]

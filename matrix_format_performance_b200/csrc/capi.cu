@@ -3,8 +3,10 @@
 #include "spmv_kernels.cuh"
 #include "spmv_stream.cuh"
 #include "spmv_lowp.cuh"
+#include "mlp.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -1238,6 +1240,67 @@ int mfp_matrix_time(const mfp_matrix *m, const void *x, void *y, uint32_t reps, 
   if (mean_s) *mean_s = sum / reps;
   if (median_s) *median_s = t[t.size() / 2];
   return ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Format selector network (engine extension)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+uint32_t mfp_mlp_param_count(void) { return d::kMlpParams; }
+
+int mfp_mlp_forward(const float *P, const float *x, uint32_t B, float *h1, float *h2, float *y, void *stream) {
+  if (B == 0) return ok();
+  if (!P || !x || !h1 || !h2 || !y) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  cudaStream_t s = as_stream(stream);
+  auto grid = [](uint64_t n) { return (uint32_t)((n + 255) / 256); };
+  d::mlp_dense_fwd<true><<<grid((uint64_t)B * d::kMlpHid), 256, 0, s>>>(x, P + d::kMlpW1, P + d::kMlpB1, h1, B,
+                                                                       d::kMlpIn, d::kMlpHid);
+  d::mlp_dense_fwd<true><<<grid((uint64_t)B * d::kMlpHid), 256, 0, s>>>(h1, P + d::kMlpW2, P + d::kMlpB2, h2, B,
+                                                                       d::kMlpHid, d::kMlpHid);
+  d::mlp_dense_fwd<false><<<grid((uint64_t)B * d::kMlpOut), 256, 0, s>>>(h2, P + d::kMlpW3, P + d::kMlpB3, y, B,
+                                                                        d::kMlpHid, d::kMlpOut);
+  return check_launch("mlp forward");
+}
+
+int mfp_mlp_backward(const float *P, const float *x, const float *h1, const float *h2, const float *y,
+                     const float *t, const float *mask, uint32_t B, float *G, float *loss, float *work,
+                     void *stream) {
+  if (!P || !G || !loss || (B && (!x || !h1 || !h2 || !y || !t || !mask || !work)))
+    return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  cudaStream_t s = as_stream(stream);
+  if (B == 0) {
+    CUDA_TRY(cudaMemsetAsync(G, 0, d::kMlpParams * sizeof(float), s), "cudaMemsetAsync");
+    CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(float), s), "cudaMemsetAsync");
+    return ok();
+  }
+  float *dY = work, *dZ2 = work + (size_t)B * d::kMlpOut, *dZ1 = dZ2 + (size_t)B * d::kMlpHid;
+  auto grid = [](uint64_t n) { return (uint32_t)((n + 255) / 256); };
+  d::mlp_loss_grad<<<1, 1024, 0, s>>>(y, t, mask, B * d::kMlpOut, dY, loss);
+  d::mlp_dense_bwd_w<<<grid(d::kMlpHid * d::kMlpOut + d::kMlpOut), 256, 0, s>>>(h2, dY, G + d::kMlpW3, G + d::kMlpB3,
+                                                                                B, d::kMlpHid, d::kMlpOut);
+  d::mlp_dense_bwd_in<<<grid((uint64_t)B * d::kMlpHid), 256, 0, s>>>(dY, P + d::kMlpW3, h2, dZ2, B, d::kMlpHid,
+                                                                      d::kMlpOut);
+  d::mlp_dense_bwd_w<<<grid(d::kMlpHid * d::kMlpHid + d::kMlpHid), 256, 0, s>>>(h1, dZ2, G + d::kMlpW2,
+                                                                                G + d::kMlpB2, B, d::kMlpHid,
+                                                                                d::kMlpHid);
+  d::mlp_dense_bwd_in<<<grid((uint64_t)B * d::kMlpHid), 256, 0, s>>>(dZ2, P + d::kMlpW2, h1, dZ1, B, d::kMlpHid,
+                                                                      d::kMlpHid);
+  d::mlp_dense_bwd_w<<<grid(d::kMlpIn * d::kMlpHid + d::kMlpHid), 256, 0, s>>>(x, dZ1, G + d::kMlpW1, G + d::kMlpB1,
+                                                                               B, d::kMlpIn, d::kMlpHid);
+  return check_launch("mlp backward");
+}
+
+int mfp_mlp_adam(float *p, const float *g, float *m, float *v, uint32_t n, float lr, float beta1, float beta2,
+                 float eps, uint32_t step, void *stream) {
+  if (n == 0) return ok();
+  if (!p || !g || !m || !v || step == 0) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
+  const float c1 = 1.f - (float)std::pow((double)beta1, (double)step);
+  const float c2 = 1.f - (float)std::pow((double)beta2, (double)step);
+  d::mlp_adam<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(p, g, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  return check_launch("mlp adam");
 }
 
 }  // extern "C"

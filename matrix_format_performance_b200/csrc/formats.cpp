@@ -409,6 +409,56 @@ int mfp_lowp_deltas(uint32_t nnz, const uint32_t *c, uint16_t *delta, uint32_t *
   return ok();
 }
 
+// ---- selector features (engine extension) ---------------------------------
+int mfp_selector_features(uint32_t rows, uint32_t cols, const uint32_t *rp, const uint32_t *ci, float *f) {
+  if (!rp || !f) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const uint32_t nnz = rp[rows];
+  if (nnz && !ci) return fail(MFP_ERROR_INVALID_VALUE, "null columns");
+  std::vector<uint32_t> len(rows);
+  double sum = 0, sq = 0;
+  uint32_t mx = 0, empty = 0;
+  uint64_t band = 0, near = 0, diag = 0, long_nnz = 0;
+  for (uint32_t r = 0; r < rows; ++r) {
+    const uint32_t l = rp[r + 1] - rp[r];
+    len[r] = l;
+    sum += l;
+    sq += (double)l * l;
+    mx = std::max(mx, l);
+    empty += l == 0;
+    if (l > 4096) long_nnz += l;
+    for (uint32_t e = rp[r]; e < rp[r + 1]; ++e) {
+      const uint64_t d = ci[e] > r ? (uint64_t)ci[e] - r : (uint64_t)r - ci[e];
+      band = std::max(band, d);
+      near += d <= 64;
+      diag += d == 0;
+    }
+  }
+  const double mean = rows ? sum / rows : 0.0;
+  const double var = rows ? std::max(0.0, sq / rows - mean * mean) : 0.0;
+  // Gini coefficient of the row lengths: sum_i (2i - n - 1) x_(i) / (n sum x)
+  double gini = 0.0;
+  if (rows && sum > 0) {
+    std::sort(len.begin(), len.end());
+    double acc = 0.0;
+    for (uint32_t i = 0; i < rows; ++i) acc += (2.0 * (i + 1) - rows - 1.0) * len[i];
+    gini = acc / ((double)rows * sum);
+  }
+  const double dim = std::max<double>(1.0, std::max(rows, cols));
+  f[0] = (float)std::log10(std::max(1u, rows));
+  f[1] = (float)std::log10(std::max(1u, cols));
+  f[2] = (float)std::log10((double)nnz + 1.0);
+  f[3] = (float)std::log2(1.0 + mean);
+  f[4] = (float)std::log2(1.0 + std::sqrt(var));
+  f[5] = (float)std::log2(1.0 + mx);
+  f[6] = (float)gini;
+  f[7] = (float)(band / dim);
+  f[8] = nnz ? (float)((double)near / nnz) : 0.f;
+  f[9] = (float)((double)diag / std::max(1u, std::min(rows, cols)));
+  f[10] = rows ? (float)((double)empty / rows) : 0.f;
+  f[11] = nnz ? (float)((double)long_nnz / nnz) : 0.f;
+  return ok();
+}
+
 int mfp_scoo_x_windows(uint32_t nnz, const uint32_t *ci, const uint32_t *sp, uint32_t slices,
                        uint32_t *win) {
   if (!sp || !win || (nnz && !ci)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");

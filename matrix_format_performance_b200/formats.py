@@ -147,13 +147,18 @@ class hybrid_matrix_class:
         self.coo_matrix = None
 
     def allocate(self, m: csr_matrix_class, percent: float) -> None:
-        w = C.c_uint32()
-        call("mfp_hybrid_width", m.rows, ptr(m.row_ptr), float(percent), C.byref(w))
-        self.allocate_width(m, w.value)
+        self.allocate_width(m, hybrid_width(m, percent))
 
     def allocate_width(self, m: csr_matrix_class, width: int) -> None:
         self.ell_matrix = ell_matrix_class(m, int(width))
         self.coo_matrix = coo_matrix_class(m, int(width))
+
+
+def hybrid_width(m: csr_matrix_class, percent: float) -> int:
+    """ELL width of hybrid_matrix_class::allocate: avg + (max - avg) * percent."""
+    w = C.c_uint32()
+    call("mfp_hybrid_width", m.rows, ptr(m.row_ptr), float(percent), C.byref(w))
+    return int(w.value)
 
 
 def row_length_quantile(m: csr_matrix_class, q: float) -> int:

@@ -14,7 +14,7 @@ from matrix_format_performance_b200._capi import MfpError, call
 def header_functions():
     src = (ROOT / "include" / "mfp_spmv.h").read_text()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = set(re.findall(r"^\s*(?:int|const char \*)\s*(mfp_\w+)\s*\(", src, flags=re.M))
+    names = set(re.findall(r"^\s*(?:int|uint32_t|const char \*)\s*(mfp_\w+)\s*\(", src, flags=re.M))
     return sorted(names)
 
 

@@ -1,0 +1,154 @@
+"""Format selector: features, the MLP's CUDA forward/backward/Adam kernels
+against a NumPy CPU reference (itself checked by finite differences), and
+training on a toy problem.
+
+The NumPy functions below are the CPU oracle of the network: plain
+restatements of a 12-64-64-28 ReLU MLP and its masked mean-squared error.
+"""
+import numpy as np
+import pytest
+
+from matrix_format_performance_b200 import selector as S
+from matrix_format_performance_b200 import synth
+
+L = [(12, 64), (64, 64), (64, 28)]
+
+
+def unpack(p):
+    out, o = [], 0
+    for k, n in L:
+        W = p[o:o + k * n].reshape(k, n)
+        o += k * n
+        b = p[o:o + n]
+        o += n
+        out.append((W, b))
+    return out
+
+
+def ref_forward(p, x):
+    (W1, b1), (W2, b2), (W3, b3) = unpack(p.astype(np.float64))
+    h1 = np.maximum(x @ W1 + b1, 0)
+    h2 = np.maximum(h1 @ W2 + b2, 0)
+    return h1, h2, h2 @ W3 + b3
+
+
+def ref_loss(p, x, t, m):
+    _, _, y = ref_forward(p, x)
+    return float((m * (y - t) ** 2).sum() / m.sum())
+
+
+def ref_grad(p, x, t, m):
+    (W1, b1), (W2, b2), (W3, b3) = unpack(p.astype(np.float64))
+    h1, h2, y = ref_forward(p, x)
+    dy = 2 * m * (y - t) / m.sum()
+    dW3, db3 = h2.T @ dy, dy.sum(0)
+    dz2 = (dy @ W3.T) * (h2 > 0)
+    dW2, db2 = h1.T @ dz2, dz2.sum(0)
+    dz1 = (dz2 @ W2.T) * (h1 > 0)
+    dW1, db1 = x.T @ dz1, dz1.sum(0)
+    return np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3.ravel(), db3])
+
+
+def _problem(B=37, seed=0):
+    rng = np.random.default_rng(seed)
+    p = S.init_params(seed)
+    p[p.size - 28:] = rng.normal(0, 0.1, 28)  # non-zero biases too
+    x = rng.normal(0, 1, (B, 12))
+    t = rng.normal(0, 1, (B, 28))
+    m = (rng.random((B, 28)) < 0.7).astype(np.float64)
+    return p, x, t, m
+
+
+def test_reference_gradient_matches_finite_differences():
+    p, x, t, m = _problem()
+    g = ref_grad(p, x, t, m)
+    rng = np.random.default_rng(1)
+    p64 = p.astype(np.float64)
+    for i in rng.choice(p.size, 40, replace=False):
+        e = np.zeros_like(p64)
+        e[i] = 1e-6
+        fd = (ref_loss(p64 + e, x, t, m) - ref_loss(p64 - e, x, t, m)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])), i
+
+
+def test_features_match_numpy():
+    m = synth.power_law(rows=5000, seed=3)
+    f = S.features(m)
+    lens = np.diff(m.row_ptr.astype(np.int64))
+    rows = np.repeat(np.arange(m.rows), lens)
+    d = np.abs(m.columns.astype(np.int64) - rows)
+    srt = np.sort(lens)
+    gini = ((2 * np.arange(1, m.rows + 1) - m.rows - 1) * srt).sum() / (m.rows * lens.sum())
+    want = [np.log10(m.rows), np.log10(m.cols), np.log10(m.nnz + 1), np.log2(1 + lens.mean()),
+            np.log2(1 + lens.std()), np.log2(1 + lens.max()), gini, d.max() / max(m.rows, m.cols),
+            (d <= 64).mean(), (d == 0).sum() / min(m.rows, m.cols), (lens == 0).mean(), lens[lens > 4096].sum() / m.nnz]
+    assert np.allclose(f, np.array(want, np.float32), rtol=1e-5, atol=1e-6)
+
+
+def test_generator_is_seeded_and_capped():
+    a, fa = S.family_matrix(7, nnz_cap=1 << 18)
+    b, fb = S.family_matrix(7, nnz_cap=1 << 18)
+    assert fa == fb and np.array_equal(a.row_ptr, b.row_ptr) and np.array_equal(a.columns, b.columns)
+    for s in range(30):
+        m, fam = S.family_matrix(s, nnz_cap=1 << 18)
+        assert m.nnz <= (1 << 18) * 1.6 + 100_000 and fam in S.FAMILIES
+        assert np.all(np.diff(m.row_ptr.astype(np.int64)) >= 0) and m.row_ptr[-1] == m.nnz
+
+
+def test_targets_and_regret():
+    times = np.array([[2.0, 1.0, np.inf, 4.0], [1.0, 1.0, 3.0, np.inf]])
+    t, mk = S.targets(times)
+    assert np.allclose(t[0], [np.log(2), 0, 0, np.log(4)]) and np.array_equal(mk[0], [1, 1, 0, 1])
+    assert np.allclose(S.regret(times, np.array([0, 2])), [2.0, 3.0])
+
+
+@pytest.mark.gpu
+def test_mlp_kernels_match_cpu_reference():
+    import torch
+    p, x, t, m = _problem(B=301, seed=4)
+    net = S.MLP(p)
+    xt = torch.from_numpy(x.astype(np.float32)).cuda()
+    h1, h2, y = net.forward(xt)
+    rh1, rh2, ry = ref_forward(p, x.astype(np.float32).astype(np.float64))
+    assert np.allclose(y.cpu().numpy(), ry, rtol=1e-4, atol=1e-4)
+    assert np.allclose(h2.cpu().numpy(), rh2, rtol=1e-4, atol=1e-4)
+    tt = torch.from_numpy(t.astype(np.float32)).cuda()
+    mt = torch.from_numpy(m.astype(np.float32)).cuda()
+    g, loss = net.backward(xt, h1, h2, y, tt, mt)
+    rg = ref_grad(p, x.astype(np.float32).astype(np.float64), t.astype(np.float32), m)
+    assert abs(loss.item() - ref_loss(p, x.astype(np.float32).astype(np.float64), t.astype(np.float32), m)) < 1e-4
+    gg = g.cpu().numpy()
+    assert np.allclose(gg, rg, rtol=1e-3, atol=1e-5 * np.abs(rg).max())
+    # deterministic: a second backward gives the same bits
+    g2, _ = net.backward(xt, h1, h2, y, tt, mt)
+    assert np.array_equal(gg.view(np.uint32), g2.cpu().numpy().view(np.uint32))
+    # Adam on the GPU against the same update in NumPy
+    p0 = net.params().astype(np.float64)
+    net.adam(lr=1e-2)
+    mm = 0.1 * gg
+    vv = 0.001 * gg.astype(np.float64) ** 2
+    want = p0 - 1e-2 * (mm / 0.1) / (np.sqrt(vv / 0.001) + 1e-8)
+    assert np.allclose(net.params(), want, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_training_fits_a_learnable_rule():
+    """A synthetic 'best slot depends on two features' data set: the trained
+    selector picks the best slot on held-out points far more often than any
+    fixed slot does (at least 80%, and 30 points above the best fixed slot)."""
+    rng = np.random.default_rng(0)
+    F = rng.normal(0, 1, (1200, 12)).astype(np.float32)
+    times = np.full((1200, 28), np.inf)
+    for j in (0, 4, 8, 16, 24):
+        times[:, j] = 1.0 + 0.3 * rng.random(1200)
+    times[F[:, 0] > 0.5, 4] = 0.3
+    times[F[:, 1] < -0.5, 16] = 0.2
+    times[(F[:, 0] <= 0.5) & (F[:, 1] >= -0.5), 8] = 0.4
+    sel = S.train(F[:1000], times[:1000], epochs=300, batch=128, lr=3e-3)
+    assert sel.history[-1] < 0.25 * sel.history[0]
+    ok = np.isfinite(times[1000:])
+    chosen = sel.choose(F[1000:], ok)
+    r = S.regret(times[1000:], chosen)
+    fixed = min(np.mean(S.regret(times[1000:], np.full(200, j)) <= 1.05) for j in (0, 4, 8, 16, 24))
+    # points next to the rule's sharp boundaries are the misses
+    assert np.mean(r <= 1.05) >= 0.8 and np.mean(r <= 1.05) > fixed + 0.3
