@@ -152,3 +152,59 @@ def test_training_fits_a_learnable_rule():
     fixed = min(np.mean(S.regret(times[1000:], np.full(200, j)) <= 1.05) for j in (0, 4, 8, 16, 24))
     # points next to the rule's sharp boundaries are the misses
     assert np.mean(r <= 1.05) >= 0.8 and np.mean(r <= 1.05) > fixed + 0.3
+
+
+DATA = __import__("pathlib").Path(S.__file__).parent / "selector_data"
+
+
+def _held_out():
+    d = np.load(DATA / "selector_dataset.npz")
+    w = S.Selector.load(DATA / "selector_weights.npz")
+    return d, w
+
+
+def test_committed_selector_meets_target_on_cpu_reference():
+    """The committed weights, evaluated with the NumPy network on the
+    committed held-out measurements: >= 90% of the held-out matrices get a
+    configuration within 5% of the exhaustive best, far above the best
+    fixed configuration."""
+    d, w = _held_out()
+    F, T = d["F_test"].astype(np.float64), d["T_test"].astype(np.float64)
+    assert len(F) == 200 and len(d["F_train"]) == 2000
+    _, _, y = ref_forward(w.params, (F - w.mu) / w.sigma)
+    chosen = np.where(np.isfinite(T), y, np.inf).argmin(axis=1)
+    r = S.regret(T, chosen)
+    assert np.mean(r <= 1.05) >= 0.9
+    Ttr = d["T_train"].astype(np.float64)
+    rel = np.where(np.isfinite(Ttr), Ttr / np.nanmin(np.where(np.isfinite(Ttr), Ttr, np.nan), axis=1, keepdims=True),
+                   np.inf)
+    fixed = int(np.argmin([np.mean(np.minimum(rel[:, j], 10.0)) for j in range(S.N_OUT)]))
+    r_fixed = S.regret(T, np.where(np.isfinite(T[:, fixed]), fixed, 0))
+    assert np.mean(r <= 1.05) > np.mean(r_fixed <= 1.05) + 0.3
+
+
+@pytest.mark.gpu
+def test_committed_selector_cuda_forward_agrees():
+    """The CUDA forward kernels pick the same configurations as the NumPy
+    network (up to exact ties) on the held-out features."""
+    d, w = _held_out()
+    F, T = d["F_test"], d["T_test"].astype(np.float64)
+    ok = np.isfinite(T)
+    g = w.choose(F, ok)
+    _, _, y = ref_forward(w.params, (F.astype(np.float64) - w.mu) / w.sigma)
+    c = np.where(ok, y, np.inf).argmin(axis=1)
+    assert np.mean(g == c) >= 0.99
+    assert np.mean(S.regret(T, g) <= 1.05) >= 0.9
+
+
+@pytest.mark.gpu
+def test_select_end_to_end_and_sweep_fallback():
+    """select() on a fresh matrix returns an admissible configuration; a matrix
+    outside the training range goes to the exhaustive sweep."""
+    _, w = _held_out()
+    m, _ = S.family_matrix(4_000_000)
+    slot, how = w.select(m)
+    assert how == "predicted" and S.admissible(m)[slot]
+    tiny = synth.uniform(50, 1, 3, seed=1).astype(np.float32)  # 50 rows: below the training range
+    slot, how = w.select(tiny, reps=2)
+    assert how == "sweep" and S.admissible(tiny)[slot]
