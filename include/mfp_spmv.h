@@ -162,7 +162,8 @@ int mfp_csr_adaptive_row_blocks(uint32_t rows, const uint32_t *row_ptr, uint32_t
 typedef enum mfp_csr_algo { MFP_CSR_SCALAR = 0, MFP_CSR_VECTOR = 1, MFP_CSR_ADAPTIVE = 2 } mfp_csr_algo;
 typedef struct mfp_csr_config {
   uint32_t long_row_threshold; /* 0 = default for the algo; UINT32_MAX = never split */
-  uint32_t vector_lanes;       /* CSR vector lanes per row: 2..32 (power of two); 0 = auto */
+  uint32_t vector_lanes;       /* CSR vector lanes per row: 2..32 (power of two); 0 = auto
+                                  (2 below a mean row length of 12, else 4) */
   uint32_t bin_nnz;            /* CSR-Adaptive elements per row bin; 0 = default */
   uint32_t piece_nnz;          /* elements per long-row piece; 0 = default (4096) */
   uint32_t assist_threshold;   /* scalar/vector: rows longer than this (and not long) are
@@ -233,14 +234,19 @@ int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const f
  * wider slices, or x_windows == NULL, gather x from global memory. */
 int mfp_scoo_x_windows(uint32_t nnz, const uint32_t *c_index, const uint32_t *slices_ptr,
                        uint32_t slices_count, uint32_t *windows);
+/* slice_order (device, slices_count entries, may be NULL = natural order):
+ * the order the CTAs take the slices in; mfp_scoo_slice_order gives the
+ * slices by element count, heaviest first (host), which shortens the tail of
+ * matrices with a few heavy slices. */
+int mfp_scoo_slice_order(uint32_t slices_count, const uint32_t *slices_ptr, uint32_t *slice_order);
 int mfp_scoo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
                       const float *values, const uint32_t *c_index, const uint32_t *r_index,
                       const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
-                      const float *x, float *y, void *stream);
+                      const uint32_t *slice_order, const float *x, float *y, void *stream);
 int mfp_scoo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
                       const double *values, const uint32_t *c_index, const uint32_t *r_index,
                       const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
-                      const double *x, double *y, void *stream);
+                      const uint32_t *slice_order, const double *x, double *y, void *stream);
 
 /* Hybrid ELL + COO — counterpart of gpu_hybrid_spmv / gpu_hybrid_atomic_spmv
  * (gpu_matrix_multiplier.cu:866-1096).  Two launches: the ELL kernel writes

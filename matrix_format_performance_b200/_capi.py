@@ -94,8 +94,9 @@ _PROTOS = {
     "mfp_workspace_error": [vp, P_u32],
     "mfp_coo_spmv_f32_noalloc": [u32, u32, u32, vp, vp, vp, vp, vp, vp],
     "mfp_scoo_x_windows": [u32, vp, vp, u32, vp],
-    "mfp_scoo_spmv_f32": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp],
-    "mfp_scoo_spmv_f64": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp],
+    "mfp_scoo_slice_order": [u32, vp, vp],
+    "mfp_scoo_spmv_f32": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp],
+    "mfp_scoo_spmv_f64": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp],
     "mfp_hybrid_workspace_bytes": [u32, u32, C.POINTER(C.c_size_t)],
     "mfp_hybrid_spmv_f32": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],
     "mfp_hybrid_spmv_f64": [u32, u32, u32, vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_size_t, vp],

@@ -39,6 +39,11 @@ namespace dev {
 #ifndef MFP_CSR_MINBLOCKS
 #define MFP_CSR_MINBLOCKS 8
 #endif
+// CTAs per SM the register-resident COO / SCOO kernels are register-limited
+// to (FP32; FP64 uses 4).
+#ifndef MFP_COO_MINBLOCKS
+#define MFP_COO_MINBLOCKS 6
+#endif
 #ifndef MFP_PIECES_FIRST
 #define MFP_PIECES_FIRST 0
 #endif
@@ -288,6 +293,167 @@ __device__ __forceinline__ void block_segmented_reduce(const T *s_prod, const ui
 
   if (!active) return;
   const bool tail_cont = (i1 < end) && (s_row[swz(i1)] == last_row);
+  if (multi) {
+    if (head_cont)
+      emit(first_row, add_rn(left, first_sum), first_row == row_first_chunk, first_row == row_last_chunk);
+    else
+      emit(first_row, first_sum, first_row == row_first_chunk, first_row == row_last_chunk);
+    if (!tail_cont) emit(last_row, cur, false, last_row == row_last_chunk);
+  } else if (!tail_cont) {
+    emit(last_row, v, last_row == row_first_chunk, last_row == row_last_chunk);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Register-resident variant for row-sorted element streams (COO tiles, the
+// hybrid's COO tail, SCOO slices).  Thread t owns the 8 consecutive elements
+// [g, g + 8) of the chunk, g = (c0 & ~7) + 8 t, clipped to [c0, c1): it loads
+// them with 16-byte loads straight into registers (consecutive threads,
+// consecutive 32-byte pieces: coalesced), issues their 8 x gathers together,
+// and runs the same thread-sequential run sums and carry scan as
+// block_segmented_reduce, without staging products and row ids through
+// shared memory.
+// ---------------------------------------------------------------------------
+template <typename T, bool VEC, typename XS>
+__device__ __forceinline__ uint32_t load_run_group(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                                   const uint32_t *__restrict__ rows, XS xs, uint32_t g,
+                                                   uint32_t c0, uint32_t c1, T (&p)[kEpt], uint32_t (&r)[kEpt],
+                                                   uint32_t &i0, uint64_t pol) {
+  static_assert(kEpt == 8, "a group is two 4-element vectors");
+  i0 = max(g, c0);
+  const uint32_t i1 = min(g + kEpt, c1);
+  if (i0 >= i1) return 0u;
+  const uint32_t cnt = i1 - i0;
+  if (VEC && cnt == kEpt) {  // i0 == g, a multiple of 8: 16-byte aligned for 4-byte types
+    T v0[4], v1[4];
+    uint32_t k0[4], k1[4], q0[4], q1[4];
+    ld_stream4(vals + i0, v0, pol);
+    ld_stream4(vals + i0 + 4, v1, pol);
+    ld_stream4(cols + i0, k0, pol);
+    ld_stream4(cols + i0 + 4, k1, pol);
+    ld_stream4(rows + i0, q0, pol);
+    ld_stream4(rows + i0 + 4, q1, pol);
+    T x0[4], x1[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x0[k] = xs(k0[k]);
+      x1[k] = xs(k1[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      p[k] = mul_rn(v0[k], x0[k]);
+      p[4 + k] = mul_rn(v1[k], x1[k]);
+      r[k] = q0[k];
+      r[4 + k] = q1[k];
+    }
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < kEpt; ++k) {
+      if (k < cnt) {
+        const uint32_t e = i0 + k;
+        r[k] = ld_stream1(rows + e, pol);
+        p[k] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+      }
+    }
+  }
+  return cnt;
+}
+
+// block_segmented_reduce over register-held runs.  cnt: the thread's element
+// count (0 = inactive); i0, i1 = i0 + cnt its element range; c0, c1 the
+// chunk; rows_g the global row ids (for the neighbours across warps and the
+// chunk's first and last rows).
+template <typename T, typename Emit, typename Gap>
+__device__ __forceinline__ void block_segmented_reduce_regs(const T (&pr)[kEpt], const uint32_t (&rw)[kEpt],
+                                                            uint32_t cnt, uint32_t i0, uint32_t c0, uint32_t c1,
+                                                            const uint32_t *__restrict__ rows_g, Emit emit,
+                                                            Gap gap, seg_scan_smem<T> &sm) {
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const bool active = cnt > 0;
+  const uint32_t i1 = i0 + cnt;
+  const uint32_t row_first_chunk = __ldg(rows_g + c0);
+  const uint32_t row_last_chunk = __ldg(rows_g + c1 - 1u);
+  uint32_t first_row = active ? rw[0] : 0u, last_row = 0u;
+  T first_sum = T(0), cur = T(0);
+  bool multi = false;
+  if (active) {
+    uint32_t r = first_row;
+    cur = pr[0];
+#pragma unroll
+    for (uint32_t k = 1; k < kEpt; ++k) {
+      if (k < cnt) {
+        const uint32_t ri = rw[k];
+        if (ri != r) {
+          if (!multi) {
+            first_sum = cur;
+            multi = true;
+          } else {
+            emit(r, cur, false, false);
+          }
+          if (ri > r + 1u) gap(r + 1u, ri);
+          r = ri;
+          cur = pr[k];
+        } else {
+          cur = add_rn(cur, pr[k]);
+        }
+      }
+    }
+    last_row = r;
+  }
+  // neighbours' rows: the previous element (i0 - 1) is the last element of
+  // thread t - 1, the next (i1) the first of thread t + 1
+  uint32_t prev_row = __shfl_up_sync(0xffffffffu, last_row, 1);
+  uint32_t next_row = __shfl_down_sync(0xffffffffu, first_row, 1);
+  if (lane == 0) prev_row = (active && i0 > c0) ? __ldg(rows_g + i0 - 1u) : 0u;
+  if (lane == 31) next_row = (active && i1 < c1) ? __ldg(rows_g + i1) : 0u;
+  const bool has_prev = active && i0 > c0, has_next = active && i1 < c1;
+  bool head_cont = false;
+  if (has_prev) {
+    head_cont = prev_row == first_row;
+    if (!head_cont && first_row > prev_row + 1u) gap(prev_row + 1u, first_row);
+  }
+  uint32_t f = (active && !multi && head_cont) ? 0u : 1u;
+  T v = active ? cur : T(0);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T ov = __shfl_up_sync(0xffffffffu, v, o);
+    const uint32_t of = __shfl_up_sync(0xffffffffu, f, o);
+    if (lane >= (uint32_t)o) {
+      if (!f) v = add_rn(ov, v);
+      f |= of;
+    }
+  }
+  if (lane == 31) {
+    sm.warp_v[warp] = v;
+    sm.warp_f[warp] = f;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = kBlock / 32;
+    T wv = lane < nw ? sm.warp_v[lane] : T(0);
+    uint32_t wf = lane < nw ? sm.warp_f[lane] : 1u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T ov = __shfl_up_sync(0xffffffffu, wv, o);
+      const uint32_t of = __shfl_up_sync(0xffffffffu, wf, o);
+      if (lane >= (uint32_t)o) {
+        if (!wf) wv = add_rn(ov, wv);
+        wf |= of;
+      }
+    }
+    const T pv = __shfl_up_sync(0xffffffffu, wv, 1);
+    const uint32_t pf = __shfl_up_sync(0xffffffffu, wf, 1);
+    if (lane < nw) {
+      sm.prefix_v[lane] = lane == 0 ? T(0) : pv;
+      sm.prefix_f[lane] = lane == 0 ? 1u : pf;
+    }
+  }
+  __syncthreads();
+  if (!f && warp > 0) v = add_rn(sm.prefix_v[warp], v);
+  T left = __shfl_up_sync(0xffffffffu, v, 1);
+  if (lane == 0) left = warp > 0 ? sm.prefix_v[warp] : T(0);
+  if (!active) return;
+  const bool tail_cont = has_next && next_row == last_row;
   if (multi) {
     if (head_cont)
       emit(first_row, add_rn(left, first_sum), first_row == row_first_chunk, first_row == row_last_chunk);
@@ -755,8 +921,6 @@ constexpr uint32_t kWaitLimit = 1u << 22;  // ~0.3 s of 64 ns sleeps
 
 template <typename T>
 struct coo_smem {
-  __align__(16) T prod[kChunkPad];
-  __align__(16) uint32_t row[kChunkPad];
   seg_scan_smem<T> scan;
   uint32_t tile;
   T first_total, last_total;
@@ -767,7 +931,7 @@ struct coo_smem {
 // without elements untouched (the COO tail of the hybrid format, after the
 // ELL kernel has written every row).
 template <typename T, bool VEC, bool ACCUM = false>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uint32_t n_rows, uint32_t nnz,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4) coo_kernel(uint32_t n_rows, uint32_t nnz,
                                                      const T *__restrict__ vals,
                                                      const uint32_t *__restrict__ cols,
                                                      const uint32_t *__restrict__ rows,
@@ -795,11 +959,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
   const uint32_t c1 = min(nnz, c0 + (uint32_t)kChunk);
   const uint32_t p = c0 > 0 ? rows[c0 - 1] : kNoRow;
   const uint32_t nx = c1 < nnz ? rows[c1] : kNoRow;
-  const uint32_t base = c0 & ~3u;  // c0 is a multiple of kChunk: base == c0
-  stage<T, VEC, true>(vals, cols, rows, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
-  __syncthreads();
-  const uint32_t off = c0 - base, n = c1 - c0;
-  const uint32_t rf = sm.row[swz(off)], rl = sm.row[swz(off + n - 1)];
+  // c0 is a multiple of kChunk: thread t owns elements c0 + 8 t .. c0 + 8 t + 7
+  T pr[kEpt];
+  uint32_t rw[kEpt], i0 = 0;
+  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + threadIdx.x * kEpt, c0, c1, pr,
+                                              rw, i0, pol);
+  const uint32_t rf = __ldg(rows + c0), rl = __ldg(rows + c1 - 1u);
   // empty rows before the first row of this tile (after the previous tile's last)
   if (!ACCUM) {
     const uint32_t lo = (p == kNoRow) ? 0u : p + 1u;
@@ -821,7 +986,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
     if (!ACCUM)
       for (uint32_t r = lo; r < hi && r < n_rows; ++r) y[r] = T(0);
   };
-  block_segmented_reduce<T>(sm.prod, sm.row, off, n, emit, gap, sm.scan);
+  block_segmented_reduce_regs<T>(pr, rw, cnt, i0, c0, c1, rows, emit, gap, sm.scan);
   __syncthreads();
   if (threadIdx.x == 0) {
     const bool first_prev = (rf == p), last_next = (rl == nx);
@@ -879,26 +1044,27 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) coo_kernel(uin
 // ---------------------------------------------------------------------------
 template <typename T>
 struct scoo_smem_static {
-  __align__(16) T prod[kChunkPad];
-  __align__(16) uint32_t row[kChunkPad];
   seg_scan_smem<T> scan;
 };
 
 template <typename T, bool VEC, bool XWIN>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,
                                                       const uint32_t *__restrict__ ridx,
                                                       const uint32_t *__restrict__ slices_ptr,
                                                       const uint32_t *__restrict__ windows,
-                                                      uint32_t max_window, const T *__restrict__ x,
-                                                      T *__restrict__ y) {
+                                                      uint32_t max_window,
+                                                      const uint32_t *__restrict__ order,
+                                                      const T *__restrict__ x, T *__restrict__ y) {
   __shared__ scoo_smem_static<T> sm;
   extern __shared__ __align__(16) unsigned char dyn[];
   T *acc = reinterpret_cast<T *>(dyn);                       // slice_size (rounded to 4)
   T *s_x = acc + ((slice_size + 3u) & ~3u);                  // max_window + 4 when XWIN
   const uint64_t pol = policy_evict_first();
-  const uint32_t s = blockIdx.x;
+  // the hardware starts blocks in index order: with `order` (slices by element
+  // count, descending) the heaviest slices start first and the tail is short
+  const uint32_t s = order ? order[blockIdx.x] : blockIdx.x;
   const uint32_t row0 = s * slice_size;
   if (row0 >= n_rows) return;
   const uint32_t nrows = min(slice_size, n_rows - row0);
@@ -921,17 +1087,20 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 8 : 6) scoo_kernel(ui
   };
   auto gap = [](uint32_t, uint32_t) {};
   for (uint32_t c0 = eb; c0 < ee;) {
-    const uint32_t base = c0 & ~3u;
-    const uint32_t c1 = min(ee, base + (uint32_t)kChunk);
-    if (XWIN && use_win)
-      stage<T, VEC, true>(vals, cidx, ridx, x_window<T>{s_x, wlo}, c0, c1, sm.prod, sm.row, pol);
-    else
-      stage<T, VEC, true>(vals, cidx, ridx, x_global<T>{x}, c0, c1, sm.prod, sm.row, pol);
-    __syncthreads();
-    block_segmented_reduce<T>(sm.prod, sm.row, c0 - base, c1 - c0, emit, gap, sm.scan);
-    __syncthreads();
+    const uint32_t base8 = c0 & ~7u;
+    const uint32_t c1 = min(ee, base8 + (uint32_t)kChunk);
+    T pr[kEpt];
+    uint32_t rw[kEpt], i0 = 0;
+    const uint32_t g = base8 + threadIdx.x * kEpt;
+    const uint32_t cnt = (XWIN && use_win)
+                             ? load_run_group<T, VEC>(vals, cidx, ridx, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
+                             : load_run_group<T, VEC>(vals, cidx, ridx, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
+    // the chunk's emits into acc[] finish before the next chunk's scan
+    // barriers, which every thread passes only after its own emits
+    block_segmented_reduce_regs<T>(pr, rw, cnt, i0, c0, c1, ridx, emit, gap, sm.scan);
     c0 = c1;
   }
+  __syncthreads();
   for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
 }
 

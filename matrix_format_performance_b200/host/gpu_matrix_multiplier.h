@@ -244,6 +244,12 @@ measurement_class gpu_scoo_spmv(bool print_diff, const scoo_matrix_class<data_ty
     std::sort(widths.begin(), widths.end());
     if (widths[(widths.size() * 9) / 10] <= cap) max_window = (std::min(cap, widths.back()) + 3u) & ~3u;
   }
+  // slices heaviest first (shortens the tail when a few slices are heavy)
+  std::vector<uint32_t> order(slices);
+  mfp_host::check(mfp_scoo_slice_order(slices, matrix.slices_ptr.get(), order.data()), "GPU SCOO");
+  mfp_host::dev_temp dord((size_t)slices * 4);
+  if (slices)
+    mfp_host::cuda_check(cudaMemcpy(dord.p, order.data(), (size_t)slices * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
   mfp_host::dev_temp dwin(max_window ? win.size() * 4 : 0);
   if (max_window)
     mfp_host::cuda_check(cudaMemcpy(dwin.p, win.data(), win.size() * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -253,12 +259,12 @@ measurement_class gpu_scoo_spmv(bool print_diff, const scoo_matrix_class<data_ty
         return sizeof(data_type) == 4
                    ? mfp_scoo_spmv_f32(meta.rows_count, meta.cols_count, slices, matrix.slice_size,
                                        (const float *)A.get(), c_index.get(), r_index.get(), sp.as<uint32_t>(),
-                                       dwin.as<uint32_t>(), max_window, (const float *)x.get(), (float *)y.get(),
-                                       nullptr)
+                                       dwin.as<uint32_t>(), max_window, dord.as<uint32_t>(),
+                                       (const float *)x.get(), (float *)y.get(), nullptr)
                    : mfp_scoo_spmv_f64(meta.rows_count, meta.cols_count, slices, matrix.slice_size,
                                        (const double *)A.get(), c_index.get(), r_index.get(), sp.as<uint32_t>(),
-                                       dwin.as<uint32_t>(), max_window, (const double *)x.get(),
-                                       (double *)y.get(), nullptr);
+                                       dwin.as<uint32_t>(), max_window, dord.as<uint32_t>(),
+                                       (const double *)x.get(), (double *)y.get(), nullptr);
       });
 }
 
