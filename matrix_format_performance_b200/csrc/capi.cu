@@ -170,8 +170,14 @@ struct mfp_csr_plan {
   double *partials = nullptr;
   uint32_t *counters = nullptr;
   uint32_t *row_blocks = nullptr;
+  uint32_t *order = nullptr;  // work items heaviest first (n_main + n_pieces)
   size_t device_bytes = 0;
 };
+
+// Launch the CSR family's work items heaviest first (1) or in index order (0).
+#ifndef MFP_CSR_ORDER
+#define MFP_CSR_ORDER 1
+#endif
 
 namespace {
 constexpr uint32_t kDefaultLong = 4096;
@@ -388,7 +394,26 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
     delete plan;
     return fail(MFP_ERROR_TOO_LARGE, "grid too large");
   }
-  if ((st = upload(&plan->pieces, pieces.data(), pieces.size(), &plan->device_bytes)) ||
+  // launch order: work items by element count, heaviest first (stable)
+  std::vector<uint32_t> order((size_t)plan->n_main + plan->n_pieces);
+  {
+    std::vector<uint64_t> cost(order.size());
+    for (uint32_t b = 0; b < plan->n_main; ++b) {
+      const uint32_t r0 = algo == MFP_CSR_ADAPTIVE ? blocks[b] : b * d::kBlock;
+      const uint32_t r1 = algo == MFP_CSR_ADAPTIVE ? blocks[b + 1] : std::min(rows, r0 + d::kBlock);
+      uint64_t c = r1 - r0;
+      for (uint32_t r = r0; r < r1; ++r) {
+        const uint32_t len = rp[r + 1] - rp[r];
+        if (len <= cfg.long_row_threshold) c += len;
+      }
+      cost[b] = c;
+    }
+    for (uint32_t k = 0; k < plan->n_pieces; ++k) cost[plan->n_main + k] = pieces[k].e1 - pieces[k].e0;
+    for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+  }
+  if ((st = upload(&plan->order, order.data(), order.size(), &plan->device_bytes)) ||
+      (st = upload(&plan->pieces, pieces.data(), pieces.size(), &plan->device_bytes)) ||
       (st = dmalloc(&plan->partials, slots, &plan->device_bytes)) ||
       (st = dmalloc(&plan->counters, nlong, &plan->device_bytes)) ||
       (st = upload(&plan->row_blocks, blocks.data(), blocks.size(), &plan->device_bytes))) {
@@ -412,6 +437,7 @@ extern "C" int mfp_csr_plan_destroy(mfp_csr_plan *plan) {
   cudaFree(plan->partials);
   cudaFree(plan->counters);
   cudaFree(plan->row_blocks);
+  cudaFree(plan->order);
   cudaFree(plan->error);
   free_stream_plan(plan->sp[0]);
   free_stream_plan(plan->sp[1]);
@@ -469,6 +495,7 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
   A.pieces = plan->pieces;
   A.partials = plan->partials;
   A.counters = plan->counters;
+  A.order = MFP_CSR_ORDER ? plan->order : nullptr;
   const bool vec = aligned16(data) && aligned16(cols);
   cudaStream_t s = as_stream(stream);
   if (plan->nnz == 0) return fill<T>(plan->rows, y, T(0), stream);

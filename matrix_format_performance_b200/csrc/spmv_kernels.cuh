@@ -646,6 +646,9 @@ struct csr_args {
   const long_piece *__restrict__ pieces;
   double *partials;
   uint32_t *counters;
+  // work item of each block index (w < n_main: row block / bin w, else piece
+  // w - n_main), heaviest first; NULL = blocks in index order
+  const uint32_t *__restrict__ order;
 };
 
 template <typename T>
@@ -844,14 +847,22 @@ template <typename T, int ALGO, bool VEC>
 __global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && ALGO != 1) ? MFP_CSR_MINBLOCKS : 6) csr_kernel(const csr_args<T> A) {
   __shared__ csr_smem<T> sm;
   const uint64_t pol = policy_evict_first();
-  // long-row pieces: first block indices (longest work starts first) or last
-  const uint32_t pb = MFP_PIECES_FIRST ? blockIdx.x : blockIdx.x - A.n_main;
-  if (MFP_PIECES_FIRST ? blockIdx.x < A.n_pieces : blockIdx.x >= A.n_main) {
-    const long_piece pc = A.pieces[pb];
+  // the hardware starts blocks in index order: with A.order the heaviest work
+  // items (by element count) start first, which shortens the tail; without
+  // it, long-row pieces take the first block indices or the last
+  uint32_t w;
+  if (A.order)
+    w = A.order[blockIdx.x];
+  else if (MFP_PIECES_FIRST)
+    w = blockIdx.x < A.n_pieces ? A.n_main + blockIdx.x : blockIdx.x - A.n_pieces;
+  else
+    w = blockIdx.x;
+  if (w >= A.n_main) {
+    const long_piece pc = A.pieces[w - A.n_main];
     run_piece<T, VEC>(pc, A.vals, A.cols, A.x, A.y, A.partials, A.counters, sm.p.a, sm.p.b, pol);
     return;
   }
-  const uint32_t b = MFP_PIECES_FIRST ? blockIdx.x - A.n_pieces : blockIdx.x;
+  const uint32_t b = w;
   if (ALGO == 2)
     csr_adaptive_main<T, VEC>(A, sm, pol, b);
   else
