@@ -90,24 +90,43 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, d
 HOST = PKG / "host"
 DRIVER = LIBDIR / "mfp_driver"
 HOST_HEADERS = ["matrix_market_reader.h", "matrix_converter.h", "scoo_matrix_class.h", "measurement_class.h",
-                "resizable_gpu_memory.h", "gpu_matrix_multiplier.h", "cpu_matrix_multiplier.h"]
+                "resizable_gpu_memory.h", "gpu_matrix_multiplier.h", "cpu_matrix_multiplier.h",
+                "cusparse_yardstick.h"]
 
 
 def host_compile(src: Path, out: Path, extra: list[str] | None = None) -> Path:
     """Compiles a C++ program against the host layer (host/*.h) and libmfp_spmv.so."""
     out.parent.mkdir(parents=True, exist_ok=True)
     deps = [src, LIB] + [HOST / h for h in HOST_HEADERS] + [ROOT / "include" / "mfp_spmv.h"]
+    if extra and "-lmfp_yardstick" in extra:
+        deps.append(YARDSTICK)
     if _stale(out, deps):
         _run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Wno-unused-parameter", f"-I{ROOT / 'include'}",
-              f"-I{HOST}", f"-I{CUDA_HOME / 'include'}", str(src), "-o", str(out), f"-L{LIBDIR}", "-lmfp_spmv",
-              f"-L{CUDA_HOME / 'lib64'}", "-lcudart_static", "-ldl", "-lrt", "-lpthread",
-              f"-Wl,-rpath,{LIBDIR}"] + (extra or []))
+              f"-I{HOST}", f"-I{CUDA_HOME / 'include'}", str(src), "-o", str(out), f"-L{LIBDIR}", "-lmfp_spmv"]
+             + (extra or []) + [f"-L{CUDA_HOME / 'lib64'}", "-lcudart_static", "-ldl", "-lrt", "-lpthread",
+                                f"-Wl,-rpath,{LIBDIR}"])
     return out
+
+
+YARDSTICK = LIBDIR / "libmfp_yardstick.so"
+
+
+def build_yardstick() -> Path:
+    """cuSPARSE yardstick (csrc/yardstick.cpp) -> lib/libmfp_yardstick.so (library code beside the engine)."""
+    src = CSRC / "yardstick.cpp"
+    if _stale(YARDSTICK, [src, ROOT / "include" / "mfp_yardstick.h"]):
+        tmp = YARDSTICK.with_suffix(".so.tmp")
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", f"-I{ROOT / 'include'}",
+              f"-I{CUDA_HOME / 'include'}", str(src), "-o", str(tmp), f"-L{CUDA_HOME / 'lib64'}", "-lcusparse",
+              "-lcudart_static", "-ldl", "-lrt", "-lpthread", f"-Wl,-rpath,{CUDA_HOME / 'lib64'}"])
+        os.replace(tmp, YARDSTICK)
+    return YARDSTICK
 
 
 def build_driver() -> Path:
     """The main.cpp-style benchmark driver (host/main.cpp) -> lib/mfp_driver."""
-    return host_compile(HOST / "main.cpp", DRIVER)
+    build_yardstick()
+    return host_compile(HOST / "main.cpp", DRIVER, ["-lmfp_yardstick"])
 
 
 def clean() -> None:

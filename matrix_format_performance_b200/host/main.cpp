@@ -6,8 +6,9 @@
 // For every Matrix Market file named in the list (one path per line), in
 // float and double: CSR conversion, the CPU CSR columns (one single-thread run
 // as the reference answer, 20 parallel runs), then 20 runs of every GPU
-// operator (CSR, CSR vector, CSR-Adaptive, ELL, COO, SCOO, hybrid with the
-// reference's 0.2 split, under both hybrid labels), averaged by
+// operator (CSR, CSR vector, CSR-Adaptive, the cuSPARSE CSR yardstick, ELL,
+// COO, SCOO, hybrid with the reference's 0.2 split, under both hybrid
+// labels), averaged by
 // measurement_class.  Results go to the reference's files in the working
 // directory: float.json / double.json (seconds), *_effective_bandwidth.json,
 // *_computational_throughput.json ([matrix file name][label]), and
@@ -20,7 +21,7 @@
 // ELL layouts more than 64x larger than the CSR layout (the engine measures
 // the other formats of such a matrix rather than dropping it).
 // Clocks are never changed: the reference's application-clock locking is not
-// built.  MKL, cuSPARSE and cusp columns are not measured.
+// built.  MKL and cusp columns are not measured.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -34,6 +35,7 @@
 #include <vector>
 
 #include "cpu_matrix_multiplier.h"
+#include "cusparse_yardstick.h"
 #include "gpu_matrix_multiplier.h"
 #include "matrix_converter.h"
 #include "matrix_market_reader.h"
@@ -114,6 +116,9 @@ std::vector<measurement_class> perform_measurement(const matrix_market::reader &
   });
   repeat([&](bool) {
     return gpu_csr_adaptive_spmv<data_type>(csr, A, col_ids, row_ptr, x_gpu, y, x.get(), reference_answer.get());
+  });
+  repeat([&](bool) {
+    return gpu_csr_cusparse_spmv<data_type>(csr, A, col_ids, row_ptr, x_gpu, y, x.get(), reference_answer.get());
   });
   if (with_ell) {
     ell_matrix_class<data_type> ell(csr);

@@ -115,7 +115,8 @@ def test_driver_runs_every_operator(tmp_path):
                        timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "ERROR" not in r.stderr, r.stderr[-2000:]
-    labels = {"CPU CSR", "CPU CSR Parallel", "GPU CSR", "GPU CSR (vector)", "GPU CSR-Adaptive", "GPU ELL",
+    labels = {"CPU CSR", "CPU CSR Parallel", "GPU CSR", "GPU CSR (vector)", "GPU CSR-Adaptive",
+              "GPU CSR (cuSparse)", "GPU ELL",
               "GPU COO", "GPU SCOO", "GPU Hybrid (TODO)", "GPU Hybrid (atomic)"}
     info = json.loads((tmp_path / "matrices_info.json").read_text())
     assert set(info) == set(mats)
