@@ -288,6 +288,21 @@ int mfp_lowp_deltas(uint32_t nnz, const uint32_t *columns, uint16_t *delta, uint
 int mfp_lowp_spmv(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row_ptr,
                   const uint16_t *q, const float *scale, const uint32_t *columns, const uint16_t *delta,
                   const uint32_t *base, const float *x, float *y, void *stream);
+/* Reduced-precision ELL (engine extension): column-major slots
+ * [k * rows + row] as gpu_ell_spmv's layout (matrix_converter.cpp:139-174),
+ * 16-bit values q (per-row scale as above), and uint32 column ids or, with
+ * index16, 16-bit offsets from the row: column = row + off - 32768
+ * (MFP_ERROR_NOT_SUPPORTED when some |column - row| > 32767).  Padding slots
+ * hold q = 0 and the row's last column.  width >= every row length.  Host
+ * builder: q and idx hold width * rows entries (idx uint16 with index16, else
+ * uint32), scale rows. */
+int mfp_lowp_ell_from_csr(int value_type, int index16, uint32_t rows, uint32_t cols, const uint32_t *row_ptr,
+                          const uint32_t *columns, const double *values, uint32_t width, uint16_t *q, void *idx,
+                          float *scale);
+/* y = A*x (device arrays; offsets or columns given, the other NULL). */
+int mfp_lowp_ell_spmv(int value_type, uint32_t rows, uint32_t cols, uint32_t width, const uint16_t *q,
+                      const float *scale, const uint32_t *columns, const uint16_t *offsets, const float *x, float *y,
+                      void *stream);
 /* Error word of the pipelined reduced-precision kernel on `device` (bit 0: a
  * stage wait gave up, the results of that launch are incomplete); `clear`
  * resets it.  Synchronous.  Engine extension, no counterpart in the reference. */
@@ -388,7 +403,8 @@ typedef enum mfp_format {
   MFP_FORMAT_COO = 4,
   MFP_FORMAT_SCOO = 5,
   MFP_FORMAT_HYBRID = 6,
-  MFP_FORMAT_CSR_LOWP = 7 /* reduced-precision CSR (engine extension) */
+  MFP_FORMAT_CSR_LOWP = 7, /* reduced-precision CSR (engine extension) */
+  MFP_FORMAT_ELL_LOWP = 8  /* reduced-precision ELL (engine extension) */
 } mfp_format;
 typedef struct mfp_matrix mfp_matrix;
 
@@ -415,6 +431,10 @@ int mfp_matrix_create_hybrid(int value_type, uint32_t rows, uint32_t cols, uint3
 int mfp_matrix_create_lowp(int value_type, int index16, uint32_t rows, uint32_t cols, uint32_t nnz,
                            const uint32_t *row_ptr, const uint32_t *columns, const double *values,
                            mfp_matrix **out);
+/* Reduced-precision ELL from host CSR with FP64 values (width = longest row). */
+int mfp_matrix_create_lowp_ell(int value_type, int index16, uint32_t rows, uint32_t cols, uint32_t nnz,
+                               const uint32_t *row_ptr, const uint32_t *columns, const double *values,
+                               mfp_matrix **out);
 int mfp_matrix_destroy(mfp_matrix *m);
 
 typedef struct mfp_matrix_info {

@@ -104,6 +104,9 @@ _PROTOS = {
     "mfp_lowp_deltas": [u32, vp, vp, vp],
     "mfp_lowp_spmv": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp],
     "mfp_lowp_error": [i32, i32, P_u32],
+    "mfp_lowp_ell_from_csr": [i32, i32, u32, u32, vp, vp, vp, u32, vp, vp, vp],
+    "mfp_lowp_ell_spmv": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp],
+    "mfp_matrix_create_lowp_ell": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(vp)],
     "mfp_matrix_create_lowp": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(vp)],
     "mfp_fill_f32": [u64, vp, C.c_float, vp],
     "mfp_fill_f64": [u64, vp, f64, vp],

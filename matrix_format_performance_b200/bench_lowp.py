@@ -2,10 +2,11 @@
 
     python -m matrix_format_performance_b200.bench_lowp [--stencil 128] [--banded 8388608] [--reps 20]
 
-For each matrix: device time of every FP32 CSR kernel (row-block scalar,
-vector, adaptive, and the streaming kernel at two chunk sizes; the fastest is
-"the FP32 plain kernel") and of the 16-bit-value CSR (BF16 and FP16, with
-uint32 column ids and with 16-bit column deltas), CUDA events around each
+For each matrix: device time of every FP32 plain kernel (CSR row-block
+scalar, vector, adaptive, the streaming CSR kernel at two chunk sizes, and
+ELL; the fastest is "the FP32 plain kernel") and of the 16-bit-value layouts
+(CSR and ELL, BF16 and FP16, with uint32 column ids and with 16-bit column
+deltas / offsets), CUDA events around each
 launch with L2 flushed before it; max and mean per-row relative error against
 the FP64 product (|y - y*| / sum_j |a_ij x_j|).  One JSON line per matrix.
 """
@@ -57,7 +58,7 @@ def fp64_product(m, x: np.ndarray, rows_per_chunk: int = 1 << 20) -> tuple[np.nd
 def measure(name: str, m64, reps: int) -> dict:
     import torch
     from . import synth
-    from .device import BF16, CSR_ADAPTIVE, CSR_SCALAR, CSR_VECTOR, F16, DeviceMatrix, device_info
+    from .device import BF16, CSR_ADAPTIVE, CSR_SCALAR, CSR_VECTOR, ELL, F16, DeviceMatrix, device_info
     dev = device_info(0)
     stream = torch.cuda.current_stream()
     flush = torch.empty(int(2 * dev.l2_bytes) // 4 + 1, device="cuda")
@@ -71,8 +72,14 @@ def measure(name: str, m64, reps: int) -> dict:
     for fmt, label, cfg in ((CSR_SCALAR, "GPU CSR", None), (CSR_VECTOR, "GPU CSR (vector)", None),
                             (CSR_ADAPTIVE, "GPU CSR-Adaptive", None),
                             (CSR_SCALAR, "GPU CSR (streaming, 2048)", {"kernel": 2}),
-                            (CSR_SCALAR, "GPU CSR (streaming, 1024)", {"kernel": 3})):
-        dm = DeviceMatrix.from_csr(m32, fmt, cfg)
+                            (CSR_SCALAR, "GPU CSR (streaming, 1024)", {"kernel": 3}), (ELL, "GPU ELL", None)):
+        if fmt == ELL:
+            from .formats import ell_matrix_class
+            if ell_matrix_class.estimate_size(m32) * 8 > (1 << 31):
+                continue
+            dm = DeviceMatrix.from_ell(ell_matrix_class(m32))
+        else:
+            dm = DeviceMatrix.from_csr(m32, fmt, cfg)
         ms = _time(dm, xt, yt, reps, flush, stream)
         info = dm.info()
         rel = np.abs(yt.cpu().numpy().astype(np.float64) - y64) / ab
@@ -82,11 +89,13 @@ def measure(name: str, m64, reps: int) -> dict:
     del m32
     base = min(v["ms"] for v in out["fp32"].values())
     out["fp32_plain_ms"] = base
-    for vt, vname in ((BF16, "BF16"), (F16, "FP16")):
-        for idx16 in (False, True):
-            key = f"{vname}{'+delta16' if idx16 else ''}"
+    for layout, vt, vname, idx16 in [(lay, vt, vn, i) for lay in ("CSR", "ELL") for vt, vn in ((BF16, "BF16"), (F16, "FP16"))
+                                     for i in (False, True)]:
+        if True:
+            key = f"{layout} {vname}{('+delta16' if layout == 'CSR' else '+offset16') if idx16 else ''}"
             try:
-                dm = DeviceMatrix.from_csr_lowp(m64, vt, idx16)
+                dm = (DeviceMatrix.from_csr_lowp(m64, vt, idx16) if layout == "CSR"
+                      else DeviceMatrix.from_ell_lowp(m64, vt, idx16))
             except Exception as e:  # 16-bit deltas need local columns
                 out["reduced"][key] = {"skipped": str(e)}
                 continue

@@ -708,6 +708,37 @@ int lowp_spmv(int vt, uint32_t rows, uint32_t nnz, const uint32_t *rp, const uin
   return check_launch("lowp_kernel launch");
 }
 
+// The 16-bit ELL kernel's VEC path (8 consecutive rows per thread, 16-byte
+// loads) when the layout allows it (1), or always the lane-interleaved path (0).
+#ifndef MFP_LOWP_ELL_VEC
+#define MFP_LOWP_ELL_VEC 1
+#endif
+int lowp_ell_spmv(int vt, uint32_t rows, uint32_t width, const uint16_t *q, const float *scale, const uint32_t *cols,
+                  const uint16_t *off, const float *x, float *y, void *stream) {
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (rows == 0) return ok();
+  if (!scale || !y || (width && (!q || !x || (!cols && !off)))) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  const bool d16 = cols == nullptr;
+  const bool vec = MFP_LOWP_ELL_VEC && rows % 8 == 0 && aligned16(q) && (d16 ? aligned16(off) : aligned16(cols));
+  cudaStream_t s = as_stream(stream);
+  const uint32_t grid = ceil_div(ceil_div(rows, 8), d::kBlock);
+#define MFP_LELL(VT, D16)                                                                         \
+  {                                                                                               \
+    d::lowp_ell_args<VT, D16> A{rows, width, q, scale, cols, off, x, y};                          \
+    if (vec)                                                                                      \
+      d::lowp_ell_kernel<VT, D16, true><<<grid, d::kBlock, 0, s>>>(A);                            \
+    else                                                                                          \
+      d::lowp_ell_kernel<VT, D16, false><<<grid, d::kBlock, 0, s>>>(A);                           \
+  }
+  if (vt == MFP_BF16) {
+    if (d16) MFP_LELL(2, true) else MFP_LELL(2, false)
+  } else {
+    if (d16) MFP_LELL(3, true) else MFP_LELL(3, false)
+  }
+#undef MFP_LELL
+  return check_launch("lowp_ell_kernel launch");
+}
+
 // Hybrid: the ELL kernel writes every row's ELL part, then the tile-based COO
 // kernel adds the tail (elements past the ELL width) row by row.
 template <typename T>
@@ -796,6 +827,10 @@ int mfp_lowp_spmv(int vt, uint32_t rows, uint32_t, uint32_t nnz, const uint32_t 
                   const float *scale, const uint32_t *cols, const uint16_t *delta, const uint32_t *base,
                   const float *x, float *y, void *s) {
   return lowp_spmv(vt, rows, nnz, rp, q, scale, cols, delta, base, x, y, s);
+}
+int mfp_lowp_ell_spmv(int vt, uint32_t rows, uint32_t, uint32_t width, const uint16_t *q, const float *scale,
+                      const uint32_t *cols, const uint16_t *off, const float *x, float *y, void *s) {
+  return lowp_ell_spmv(vt, rows, width, q, scale, cols, off, x, y, s);
 }
 int mfp_lowp_error(int device, int clear, uint32_t *error) {
   if (!error) return fail(MFP_ERROR_INVALID_VALUE, "null output");
@@ -1167,17 +1202,57 @@ int mfp_matrix_create_lowp(int vt, int index16, uint32_t rows, uint32_t cols, ui
   return finish_matrix(m, out);
 }
 
+int mfp_matrix_create_lowp_ell(int vt, int index16, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
+                               const uint32_t *ci, const double *v, mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (nnz && (!ci || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  int st = check_row_ptr(rows, nnz, rp);
+  if (st) return st;
+  if ((st = check_columns(ci, nnz, cols))) return st;
+  uint32_t width = 0;
+  for (uint32_t r = 0; r < rows; ++r) width = std::max(width, rp[r + 1] - rp[r]);
+  const uint64_t slots = (uint64_t)width * rows;
+  if (slots > (uint64_t)1 << 33) return fail(MFP_ERROR_TOO_LARGE, "ELL padding: %llu slots", (unsigned long long)slots);
+  std::vector<uint16_t> q(slots), off(index16 ? slots : 0);
+  std::vector<uint32_t> c32(index16 ? 0 : slots);
+  std::vector<float> sc(rows);
+  if ((st = mfp_lowp_ell_from_csr(vt, index16, rows, cols, rp, ci, v, width, q.data(),
+                                  index16 ? (void *)off.data() : (void *)c32.data(), sc.data())))
+    return st;
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = MFP_FORMAT_ELL_LOWP;
+  m->value_type = MFP_F32;  // x and y
+  m->lowp_vt = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  m->width = width;
+  m->format_bytes = slots * (index16 ? 4 : 6) + (uint64_t)rows * 4 + (uint64_t)cols * 4 + (uint64_t)rows * 4;
+  if ((st = track_upload(m, &m->scale, sc.data(), sc.size())) ||
+      (st = track_upload_bytes(m, &m->vals, q.data(), q.size() * 2)) ||
+      (index16 ? (st = track_upload(m, &m->delta, off.data(), off.size()))
+               : (st = track_upload(m, &m->cols_a, c32.data(), c32.size())))) {
+    mfp_matrix_destroy(m);
+    return st;
+  }
+  return finish_matrix(m, out);
+}
+
 int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
   if (!m || !out) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   const size_t vs = value_size(m->value_type);
   out->format = m->format;
-  out->value_type = m->format == MFP_FORMAT_CSR_LOWP ? m->lowp_vt : m->value_type;
+  const bool lowp = m->format == MFP_FORMAT_CSR_LOWP || m->format == MFP_FORMAT_ELL_LOWP;
+  out->value_type = lowp ? m->lowp_vt : m->value_type;
   out->rows = m->rows;
   out->cols = m->cols;
   out->nnz = m->nnz;
   out->format_bytes = m->format_bytes;
   out->algorithmic_bytes = m->nnz * (vs + 4) + ((uint64_t)m->rows + 1) * 4 + (uint64_t)m->cols * vs + (uint64_t)m->rows * vs;
-  if (m->format == MFP_FORMAT_CSR_LOWP)  // 16-bit values, uint32 column ids, row scales
+  if (lowp)  // 16-bit values, uint32 column ids, row scales
     out->algorithmic_bytes = m->nnz * 6 + (uint64_t)m->rows * 4 + ((uint64_t)m->rows + 1) * 4 +
                              (uint64_t)m->cols * 4 + (uint64_t)m->rows * 4;
   out->device_bytes = m->device_bytes;
@@ -1219,6 +1294,9 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                  : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
                                    (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
                                    m->ws_bytes, stream);
+    case MFP_FORMAT_ELL_LOWP:
+      return lowp_ell_spmv(m->lowp_vt, m->rows, m->width, (const uint16_t *)m->vals, m->scale,
+                           m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);
     case MFP_FORMAT_CSR_LOWP:
       return lowp_spmv(m->lowp_vt, m->rows, (uint32_t)m->nnz, m->rows_a, (const uint16_t *)m->vals, m->scale,
                        m->delta ? nullptr : m->cols_a, m->delta, m->base, (const float *)x, (float *)y, stream);

@@ -409,6 +409,42 @@ int mfp_lowp_deltas(uint32_t nnz, const uint32_t *c, uint16_t *delta, uint32_t *
   return ok();
 }
 
+int mfp_lowp_ell_from_csr(int vt, int index16, uint32_t rows, uint32_t cols, const uint32_t *rp, const uint32_t *ci,
+                          const double *v, uint32_t width, uint16_t *q, void *idx, float *scale) {
+  if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
+  if (!rp || !scale || ((uint64_t)width * rows && (!q || !idx))) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  const uint32_t nnz = rp[rows];
+  if (nnz && (!ci || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  for (uint32_t r = 0; r < rows; ++r)
+    if (rp[r + 1] - rp[r] > width) return fail(MFP_ERROR_INVALID_VALUE, "row %u longer than the width %u", r, width);
+  std::vector<uint16_t> qc(nnz);
+  int st = mfp_lowp_quantize(vt, rows, rp, v, qc.data(), scale);
+  if (st) return st;
+  uint16_t *off = static_cast<uint16_t *>(idx);
+  uint32_t *c32 = static_cast<uint32_t *>(idx);
+  const size_t stride = rows;
+  for (uint32_t r = 0; r < rows; ++r) {
+    const uint32_t b = rp[r], len = rp[r + 1] - b;
+    // a padding slot gathers a column its row already reads (or the diagonal)
+    const uint32_t pad_col = len ? ci[b + len - 1] : (r < cols ? r : 0u);
+    for (uint32_t k = 0; k < width; ++k) {
+      const size_t o = (size_t)k * stride + r;
+      const uint32_t c = k < len ? ci[b + k] : pad_col;
+      q[o] = k < len ? qc[b + k] : uint16_t(0);
+      if (index16) {
+        const int64_t d = (int64_t)c - (int64_t)r;
+        if (d < -32768 || d > 32767)
+          return fail(MFP_ERROR_NOT_SUPPORTED, "16-bit column offsets: row %u column %u is %lld away", r, c,
+                      (long long)d);
+        off[o] = (uint16_t)(d + 32768);
+      } else {
+        c32[o] = c;
+      }
+    }
+  }
+  return ok();
+}
+
 // ---- selector features (engine extension) ---------------------------------
 int mfp_selector_features(uint32_t rows, uint32_t cols, const uint32_t *rp, const uint32_t *ci, float *f) {
   if (!rp || !f) return fail(MFP_ERROR_INVALID_VALUE, "null argument");

@@ -513,5 +513,107 @@ __global__ void __launch_bounds__(kLowpThreads, 3) lowp_tma_kernel(const lowp_ar
   }
 }
 
+// ---------------------------------------------------------------------------
+// Reduced-precision ELL: column-major slots [k * rows + row] (the reference's
+// ELL order), 16-bit values q with one FP32 scale per row, and either uint32
+// column ids or 16-bit column offsets from the row (col = row + off - 32768).
+// Padding slots hold q = 0 and a column of their row.  A thread owns 8 rows:
+// VEC (rows % 8 == 0, 16-byte-aligned arrays) 8 consecutive rows, one 16-byte
+// load of 8 values and one of 8 offsets (or two of ids) per slot; otherwise 8
+// rows interleaved across its warp (row = warp base + 32 j + lane), so each
+// 2-byte load and each x gather is contiguous over the warp.  Slots in order
+// 0..width-1, FMA accumulation; y = acc * scale.
+// ---------------------------------------------------------------------------
+template <int VT, bool D16>
+struct lowp_ell_args {
+  uint32_t n_rows, width;
+  const uint16_t *__restrict__ q;
+  const float *__restrict__ scale;
+  const uint32_t *__restrict__ cols;  // !D16
+  const uint16_t *__restrict__ off;   // D16
+  const float *__restrict__ x;
+  float *__restrict__ y;
+};
+
+template <int VT, bool D16, bool VEC>
+__global__ void __launch_bounds__(kBlock) lowp_ell_kernel(const lowp_ell_args<VT, D16> A) {
+  const uint64_t pol = policy_evict_first();
+  const size_t stride = A.n_rows;
+  if (VEC) {
+    const uint32_t r = (blockIdx.x * kBlock + threadIdx.x) * 8u;
+    if (r >= A.n_rows) return;
+    float acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+#pragma unroll 2
+    for (uint32_t k = 0; k < A.width; ++k) {
+      const size_t o = (size_t)k * stride + r;
+      uint32_t qv[4], c[8];
+      ld_stream8_u16(A.q + o, qv, pol);
+      if (D16) {
+        uint32_t dv[4];
+        ld_stream8_u16(A.off + o, dv, pol);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          c[2 * j] = r + 2u * j + (dv[j] & 0xffffu) - 32768u;
+          c[2 * j + 1] = r + 2u * j + 1u + (dv[j] >> 16) - 32768u;
+        }
+      } else {
+        uint32_t c0[4], c1[4];
+        ld_stream4(A.cols + o, c0, pol);
+        ld_stream4(A.cols + o + 4, c1, pol);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          c[j] = c0[j];
+          c[4 + j] = c1[j];
+        }
+      }
+      float xv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) xv[j] = ld_x(A.x + c[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float2 f = lowp_pair<VT>(qv[j]);
+        acc[2 * j] = __fmaf_rn(f.x, xv[2 * j], acc[2 * j]);
+        acc[2 * j + 1] = __fmaf_rn(f.y, xv[2 * j + 1], acc[2 * j + 1]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) A.y[r + j] = acc[j] * A.scale[r + j];
+  } else {
+    // 8 rows per thread, interleaved across the warp: row = warp base + 32 j +
+    // lane, so every load and every x gather of a warp is contiguous
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t wbase = (blockIdx.x * kBlock + (threadIdx.x & ~31u)) * 8u;
+    if (wbase >= A.n_rows) return;
+    float acc[8];
+    bool ok[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc[j] = 0.f;
+      ok[j] = wbase + 32u * j + lane < A.n_rows;
+    }
+    for (uint32_t k = 0; k < A.width; ++k) {
+      const size_t o = (size_t)k * stride + wbase + lane;
+      uint32_t qv[8], c[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t r = wbase + 32u * j + lane;
+        qv[j] = ok[j] ? ld_stream_u16(A.q + o + 32u * j, pol) : 0u;
+        c[j] = ok[j] ? (D16 ? r + ld_stream_u16(A.off + o + 32u * j, pol) - 32768u : ld_stream1(A.cols + o + 32u * j, pol))
+                     : 0u;
+      }
+      float xv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) xv[j] = ok[j] ? ld_x(A.x + c[j]) : 0.f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] = __fmaf_rn(lowp_to_float<VT>(qv[j]), xv[j], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (ok[j]) A.y[wbase + 32u * j + lane] = acc[j] * A.scale[wbase + 32u * j + lane];
+  }
+}
+
 }  // namespace dev
 }  // namespace mfp

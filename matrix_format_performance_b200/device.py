@@ -17,7 +17,7 @@ from ._capi import call
 from .formats import (coo_matrix_class, csr_matrix_class, ell_matrix_class, hybrid_matrix_class, ptr,
                       scoo_matrix_class)
 
-CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID, CSR_LOWP = range(8)
+CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID, CSR_LOWP, ELL_LOWP = range(9)
 BF16, F16 = 2, 3
 FORMAT_NAMES = {"csr": CSR_SCALAR, "csr_vector": CSR_VECTOR, "csr_adaptive": CSR_ADAPTIVE, "ell": ELL,
                 "coo": COO, "scoo": SCOO, "hybrid": HYBRID}
@@ -25,7 +25,7 @@ FORMAT_NAMES = {"csr": CSR_SCALAR, "csr_vector": CSR_VECTOR, "csr_adaptive": CSR
 # csr_adaptive_spmv.cu:320; scoo_spmv.cu:221)
 LABELS = {CSR_SCALAR: "GPU CSR", CSR_VECTOR: "GPU CSR (vector)", CSR_ADAPTIVE: "GPU CSR-Adaptive", ELL: "GPU ELL",
           COO: "GPU COO", SCOO: "GPU SCOO", HYBRID: "GPU Hybrid (atomic)",
-          CSR_LOWP: "GPU CSR (16-bit values)"}
+          CSR_LOWP: "GPU CSR (16-bit values)", ELL_LOWP: "GPU ELL (16-bit values)"}
 _VT = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}
 
 
@@ -106,6 +106,18 @@ class DeviceMatrix:
              ptr(m.columns), ptr(v), C.byref(h))
         dm = cls(h, CSR_LOWP, np.float32)
         dm.label = f"GPU CSR ({'BF16' if value_type == BF16 else 'FP16'}{', 16-bit deltas' if index16 else ''})"
+        return dm
+
+    @classmethod
+    def from_ell_lowp(cls, m: csr_matrix_class, value_type: int = BF16, index16: bool = False) -> "DeviceMatrix":
+        """ELL with 16-bit values and per-row FP32 scales (width = longest row);
+        index16: 16-bit column offsets from the row."""
+        v = np.ascontiguousarray(m.data, np.float64)
+        h = C.c_void_p()
+        call("mfp_matrix_create_lowp_ell", value_type, int(index16), m.rows, m.cols, m.nnz, ptr(m.row_ptr),
+             ptr(m.columns), ptr(v), C.byref(h))
+        dm = cls(h, ELL_LOWP, np.float32)
+        dm.label = f"GPU ELL ({'BF16' if value_type == BF16 else 'FP16'}{', 16-bit offsets' if index16 else ''})"
         return dm
 
     @classmethod

@@ -175,3 +175,61 @@ def test_lowp_pipelined_and_row_block(oracle_lib, name, vt, index16):
     err = C.c_uint32(1)
     call("mfp_lowp_error", 0, 1, C.byref(err))
     assert err.value == 0
+
+
+# ---- reduced-precision ELL --------------------------------------------------
+def _lowp_ell_host(m, vt, index16):
+    w = int(np.diff(m.row_ptr.astype(np.int64)).max()) if m.rows else 0
+    q = np.empty(w * m.rows, np.uint16)
+    idx = np.empty(w * m.rows, np.uint16 if index16 else np.uint32)
+    sc = np.empty(m.rows, np.float32)
+    v = np.ascontiguousarray(m.data, np.float64)
+    call("mfp_lowp_ell_from_csr", vt, int(index16), m.rows, m.cols, F.ptr(m.row_ptr), F.ptr(m.columns), F.ptr(v), w,
+         F.ptr(q), F.ptr(idx), F.ptr(sc))
+    return w, q, idx, sc
+
+
+@pytest.mark.parametrize("index16", [False, True])
+def test_lowp_ell_layout_decodes_to_the_quantized_csr(index16):
+    m = synth.uniform(3_001, 0, 9, seed=21)  # empty rows, rows % 8 != 0
+    w, q, idx, sc = _lowp_ell_host(m, BF16, index16)
+    qc, scc = F.lowp_quantize(m, BF16)
+    assert np.array_equal(sc, scc)
+    lens = np.diff(m.row_ptr.astype(np.int64))
+    for r in range(0, m.rows, 97):
+        for k in range(w):
+            o = k * m.rows + r
+            col = (r + int(idx[o]) - 32768) if index16 else int(idx[o])
+            if k < lens[r]:
+                e = m.row_ptr[r] + k
+                assert q[o] == qc[e] and col == m.columns[e]
+            else:
+                assert q[o] == 0 and 0 <= col < m.cols
+
+
+def test_lowp_ell_offset_limit():
+    m = synth.uniform(40_000, 1, 3, seed=22)  # columns anywhere: offsets beyond 16 bits
+    with pytest.raises(MfpError, match="16-bit column offsets"):
+        _lowp_ell_host(m, BF16, True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["stencil_32", "banded_100k", "sparse_ragged", "tiny"])
+@pytest.mark.parametrize("vt", [BF16, F16])
+@pytest.mark.parametrize("index16", [False, True])
+def test_lowp_ell_accuracy(oracle_lib, name, vt, index16):
+    import torch
+    from matrix_format_performance_b200.device import DeviceMatrix
+    m = case(name)
+    x = synth.vector(0, m.cols).astype(np.float32)
+    try:
+        dm = DeviceMatrix.from_ell_lowp(m, vt, index16)
+    except MfpError as e:  # offsets only for local columns
+        assert index16 and "16-bit column offsets" in str(e)
+        return
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.full((m.rows,), float("nan"), device="cuda")
+    dm.spmv(xt, yt)
+    torch.cuda.synchronize()
+    _check(oracle_lib, m, vt, yt.cpu().numpy(), x)
+    assert dm.info().value_type == vt
