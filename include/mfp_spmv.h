@@ -149,6 +149,59 @@ int mfp_csr_adaptive_row_blocks(uint32_t rows, const uint32_t *row_ptr, uint32_t
                                 uint32_t *row_blocks, uint32_t *count);
 
 /* ------------------------------------------------------------------------- */
+/* On-device format conversion (engine extension of the host converters     */
+/* above): the same layouts, identical arrays, built by CUDA kernels from    */
+/* DEVICE arrays.  Functions that return a count or a status found on the    */
+/* device wait for `stream`; the others only enqueue work on it.             */
+/* ------------------------------------------------------------------------- */
+
+/* get_rows_statistics of a device row_ptr (waits).  Bit-identical to
+ * mfp_get_rows_statistics: the std deviation comes from an exact integer sum
+ * of squared deviations, or from the host loop when that sum reaches 2^53. */
+int mfp_dev_rows_statistics(uint32_t rows, const uint32_t *row_ptr, mfp_rows_statistic *out, void *stream);
+/* Validates a device CSR (waits): row_ptr[0] = 0, non-decreasing,
+ * row_ptr[rows] = nnz, every column < cols. */
+int mfp_dev_check_csr(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row_ptr,
+                      const uint32_t *columns, void *stream);
+/* mfp_coo_count on the device (waits). */
+int mfp_dev_coo_count(uint32_t rows, const uint32_t *row_ptr, uint32_t element_start, uint32_t *count,
+                      void *stream);
+/* coo_matrix_class (matrix_converter.cpp:211-280) from a device CSR; outputs
+ * sized mfp_dev_coo_count(element_start).  value_type MFP_F32 / MFP_F64.
+ * Waits for the output size when element_start > 0 or to read row_ptr[rows]. */
+int mfp_dev_coo_from_csr(int value_type, uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const void *data, uint32_t element_start, void *coo_data, uint32_t *coo_cols,
+                         uint32_t *coo_rows, void *stream);
+/* ell_matrix_class (matrix_converter.cpp:139-203) from a device CSR:
+ * column-major, padding col 0 / value 0; outputs sized width*rows. */
+int mfp_dev_ell_from_csr(int value_type, uint32_t rows, const uint32_t *row_ptr, const uint32_t *columns,
+                         const void *data, uint32_t width, void *ell_data, uint32_t *ell_columns,
+                         void *stream);
+/* scoo_matrix_class (scoo_matrix_class.cpp:58-100) from a device CSR with the
+ * parameters of mfp_scoo_params_compute; slices_ptr sized slices_count+1. */
+int mfp_dev_scoo_from_csr(int value_type, uint32_t rows, uint32_t nnz, const uint32_t *row_ptr,
+                          const uint32_t *columns, const void *data, const mfp_scoo_params *params,
+                          void *values, uint32_t *c_index, uint32_t *r_index, uint32_t *slices_ptr,
+                          void *stream);
+/* mfp_scoo_x_windows on the device: [min col, max col + 1) per slice. */
+int mfp_dev_scoo_x_windows(uint32_t nnz, const uint32_t *c_index, const uint32_t *slices_ptr, uint32_t slices,
+                           uint32_t *windows, void *stream);
+/* csr_matrix_class(matrix_market::matrix_class) (matrix_converter.cpp:15-87)
+ * from device COO triplets in any order (waits): row_ptr by histogram and
+ * scan, elements ordered by (row, column) with a stable radix sort, so
+ * repeated (row, column) entries keep their input order like
+ * mfp_csr_from_coo.  Out-of-range ids return MFP_ERROR_INVALID_VALUE. */
+int mfp_dev_csr_from_coo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row_ids,
+                         const uint32_t *col_ids, const double *values, uint32_t *row_ptr, uint32_t *columns,
+                         void *data, void *stream);
+/* The converters' scratch comes from a memory pool of the current device that
+ * keeps freed scratch mapped for the next conversion.  scratch_bytes reports
+ * what the pool holds; scratch_release waits for the device and returns the
+ * unused part to the driver. */
+int mfp_dev_scratch_bytes(uint64_t *reserved);
+int mfp_dev_scratch_release(void);
+
+/* ------------------------------------------------------------------------- */
 /* Device-pointer SpMV entry points: y = A * x, enqueued on `stream`.        */
 /* ------------------------------------------------------------------------- */
 
@@ -435,6 +488,19 @@ int mfp_matrix_create_lowp(int value_type, int index16, uint32_t rows, uint32_t 
 int mfp_matrix_create_lowp_ell(int value_type, int index16, uint32_t rows, uint32_t cols, uint32_t nnz,
                                const uint32_t *row_ptr, const uint32_t *columns, const double *values,
                                mfp_matrix **out);
+/* Any of formats 0..6 from a DEVICE CSR (row_ptr, columns, data on the
+ * current device), converted on the GPU with the mfp_dev_* functions; the
+ * caller keeps its arrays.  options may be NULL: CSR defaults, ELL width =
+ * longest row, SCOO parameters for the current device. */
+#define MFP_ELL_WIDTH_LONGEST 0xFFFFFFFFu
+typedef struct mfp_device_build_options {
+  const mfp_csr_config *csr;   /* CSR family launch configuration (NULL = defaults) */
+  uint32_t ell_width;          /* ELL / hybrid ELL part: slots per row, or MFP_ELL_WIDTH_LONGEST */
+  const mfp_scoo_params *scoo; /* SCOO parameters (NULL = mfp_scoo_params_compute for this device) */
+} mfp_device_build_options;
+int mfp_matrix_create_device(int format, int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
+                             const uint32_t *row_ptr, const uint32_t *columns, const void *data,
+                             const mfp_device_build_options *options, mfp_matrix **out);
 int mfp_matrix_destroy(mfp_matrix *m);
 
 typedef struct mfp_matrix_info {

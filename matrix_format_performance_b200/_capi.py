@@ -190,3 +190,24 @@ _PROTOS.update({
     "mfp_mlp_adam": [vp, vp, vp, vp, u32, C.c_float, C.c_float, C.c_float, C.c_float, u32, vp],
 })
 _RESTYPES["mfp_mlp_param_count"] = u32
+
+
+class DeviceBuildOptions(C.Structure):
+    _fields_ = [("csr", C.POINTER(CsrConfig)), ("ell_width", u32), ("scoo", C.POINTER(ScooParams))]
+
+
+ELL_WIDTH_LONGEST = 0xFFFFFFFF
+_PROTOS.update({
+    "mfp_dev_rows_statistics": [u32, vp, C.POINTER(RowsStatistic), vp],
+    "mfp_dev_check_csr": [u32, u32, u32, vp, vp, vp],
+    "mfp_dev_coo_count": [u32, vp, u32, P_u32, vp],
+    "mfp_dev_coo_from_csr": [i32, u32, vp, vp, vp, u32, vp, vp, vp, vp],
+    "mfp_dev_ell_from_csr": [i32, u32, vp, vp, vp, u32, vp, vp, vp],
+    "mfp_dev_scoo_from_csr": [i32, u32, u32, vp, vp, vp, C.POINTER(ScooParams), vp, vp, vp, vp, vp],
+    "mfp_dev_scoo_x_windows": [u32, vp, vp, u32, vp, vp],
+    "mfp_dev_csr_from_coo": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp],
+    "mfp_dev_scratch_bytes": [C.POINTER(u64)],
+    "mfp_dev_scratch_release": [],
+    "mfp_matrix_create_device": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(DeviceBuildOptions),
+                                 C.POINTER(vp)],
+})

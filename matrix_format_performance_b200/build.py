@@ -26,7 +26,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["capi.cu"]
+CU_SOURCES = ["capi.cu", "convert.cu"]
 CPP_SOURCES = ["util.cpp", "formats.cpp", "synth.cpp"]
 HEADERS = ["spmv_device.cuh", "spmv_kernels.cuh", "spmv_stream.cuh", "spmv_lowp.cuh", "mlp.cuh", "host_common.h"]
 

@@ -933,6 +933,41 @@ int finish_matrix(mfp_matrix *m, mfp_matrix **out) {
   return ok();
 }
 bool valid_vt(int vt) { return vt == MFP_F32 || vt == MFP_F64; }
+int track_bytes(mfp_matrix *m, void **p, size_t bytes) {
+  unsigned char *q = nullptr;
+  const int st = track(m, &q, bytes);
+  *p = q;
+  return st;
+}
+
+// SCOO x windows ([lo, hi) column range per slice, host copy) and slice order:
+// a slice's x window is staged in shared memory when 90% of the windows fit;
+// slices launch heaviest first.
+int scoo_attach_windows(mfp_matrix *m, const std::vector<uint32_t> &win, const uint32_t *sp_host) {
+  const size_t vs = value_size(m->value_type);
+  std::vector<uint32_t> widths;
+  for (uint32_t s = 0; s < m->slices; ++s)
+    if (win[2 * s + 1] > win[2 * s]) widths.push_back(win[2 * s + 1] - win[2 * s]);
+  const uint32_t cap = (uint32_t)((m->value_type == MFP_F64 ? 48u : 96u) * 1024u / vs);
+  bool use_win = false;
+  if (!widths.empty()) {
+    std::sort(widths.begin(), widths.end());
+    const uint32_t p90 = widths[(widths.size() * 9) / 10];
+    if (p90 <= cap) {
+      use_win = true;
+      m->max_window = std::min(cap, widths.back());
+      m->max_window = (m->max_window + 3u) & ~3u;
+    }
+  }
+  int st;
+  if (use_win && (st = track_upload(m, &m->win, win.data(), win.size()))) return st;
+  std::vector<uint32_t> order(m->slices);
+  if ((st = mfp_scoo_slice_order(m->slices, sp_host, order.data())) ||
+      (st = track_upload(m, &m->order, order.data(), order.size())))
+    return st;
+  return MFP_SUCCESS;
+}
+
 int check_columns(const uint32_t *c, uint64_t n, uint32_t cols) {
   for (uint64_t i = 0; i < n; ++i)
     if (c[i] >= cols && !(cols == 0 && c[i] == 0))
@@ -1081,33 +1116,12 @@ int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, c
   m->slices = prm->slices_count;
   m->slice_size = prm->slice_size;
   m->format_bytes = (uint64_t)nnz * (vs + 8) + ((uint64_t)m->slices + 1) * 4 + (uint64_t)cols * vs + (uint64_t)rows * vs;
-  // x windows: stage a slice's x window in shared memory when most windows fit
   std::vector<uint32_t> win(2 * (size_t)m->slices);
   mfp_scoo_x_windows(nnz, ci, sp, m->slices, win.data());
-  std::vector<uint32_t> widths;
-  for (uint32_t s = 0; s < m->slices; ++s)
-    if (win[2 * s + 1] > win[2 * s]) widths.push_back(win[2 * s + 1] - win[2 * s]);
-  const uint32_t cap = (uint32_t)((vt == MFP_F64 ? 48u : 96u) * 1024u / vs);
-  bool use_win = false;
-  if (!widths.empty()) {
-    std::sort(widths.begin(), widths.end());
-    const uint32_t p90 = widths[(widths.size() * 9) / 10];
-    if (p90 <= cap) {
-      use_win = true;
-      m->max_window = std::min(cap, widths.back());
-      m->max_window = (m->max_window + 3u) & ~3u;
-    }
-  }
   int st;
   if ((st = track_upload_bytes(m, &m->vals, v, (size_t)nnz * vs)) || (st = track_upload(m, &m->cols_a, ci, nnz)) ||
       (st = track_upload(m, &m->rows_a, ri, nnz)) || (st = track_upload(m, &m->aux, sp, (size_t)m->slices + 1)) ||
-      (use_win && (st = track_upload(m, &m->win, win.data(), win.size())))) {
-    mfp_matrix_destroy(m);
-    return st;
-  }
-  std::vector<uint32_t> order(m->slices);
-  if ((st = mfp_scoo_slice_order(m->slices, sp, order.data())) ||
-      (st = track_upload(m, &m->order, order.data(), order.size()))) {
+      (st = scoo_attach_windows(m, win, sp))) {
     mfp_matrix_destroy(m);
     return st;
   }
@@ -1160,6 +1174,134 @@ int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t widt
     mfp_matrix_destroy(m);
     return fail(MFP_ERROR_CUDA, "cudaMemset workspace");
   }
+  return finish_matrix(m, out);
+}
+
+// Builds a handle from a device CSR: the format's arrays are produced on the
+// GPU by the mfp_dev_* converters; only per-plan metadata comes to the host
+// (row_ptr for CSR plans, slices_ptr and x windows for SCOO).
+int mfp_matrix_create_device(int format, int vt, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *rp,
+                             const uint32_t *ci, const void *data, const mfp_device_build_options *opt,
+                             mfp_matrix **out) {
+  if (!out) return fail(MFP_ERROR_INVALID_VALUE, "null output");
+  *out = nullptr;
+  if (format < 0 || format > MFP_FORMAT_HYBRID || !valid_vt(vt))
+    return fail(MFP_ERROR_INVALID_VALUE, "bad format or value type");
+  if (nnz && (!ci || !data)) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  int st = mfp_dev_check_csr(rows, cols, nnz, rp, ci, nullptr);
+  if (st) return st;
+  const mfp_device_build_options o = opt ? *opt : mfp_device_build_options{nullptr, MFP_ELL_WIDTH_LONGEST, nullptr};
+  const size_t vs = value_size(vt);
+  auto *m = new mfp_matrix();
+  cudaGetDevice(&m->device);
+  m->format = format;
+  m->value_type = vt;
+  m->rows = rows;
+  m->cols = cols;
+  m->nnz = nnz;
+  auto bail = [&](int status) {
+    mfp_matrix_destroy(m);
+    return status;
+  };
+  uint32_t width = o.ell_width;
+  if ((format == MFP_FORMAT_ELL || format == MFP_FORMAT_HYBRID) && width == MFP_ELL_WIDTH_LONGEST) {
+    mfp_rows_statistic rs{};
+    if (rows && (st = mfp_dev_rows_statistics(rows, rp, &rs, nullptr))) return bail(st);
+    width = rows ? rs.max_elements_in_rows : 0u;
+  }
+  const uint64_t xy_bytes = (uint64_t)cols * vs + (uint64_t)rows * vs;
+  switch (format) {
+    case MFP_FORMAT_CSR_SCALAR:
+    case MFP_FORMAT_CSR_VECTOR:
+    case MFP_FORMAT_CSR_ADAPTIVE: {
+      m->format_bytes = (uint64_t)nnz * (vs + 4) + ((uint64_t)rows + 1) * 4 + xy_bytes;
+      std::vector<uint32_t> hrp((size_t)rows + 1);
+      if ((st = track_bytes(m, &m->vals, (size_t)nnz * vs)) ||
+          (st = track(m, &m->cols_a, nnz)) || (st = track(m, &m->rows_a, (size_t)rows + 1)))
+        return bail(st);
+      if ((nnz && (cudaMemcpy(m->vals, data, (size_t)nnz * vs, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+                   cudaMemcpy(m->cols_a, ci, (size_t)nnz * 4, cudaMemcpyDeviceToDevice) != cudaSuccess)) ||
+          cudaMemcpy(m->rows_a, rp, hrp.size() * 4, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+          cudaMemcpy(hrp.data(), rp, hrp.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return bail(fail(MFP_ERROR_CUDA, "cudaMemcpy CSR arrays"));
+      if ((st = mfp_csr_plan_create(rows, cols, nnz, hrp.data(), format, o.csr, &m->plan))) return bail(st);
+      m->device_bytes += m->plan->device_bytes;
+      break;
+    }
+    case MFP_FORMAT_ELL: {
+      const uint64_t slots = (uint64_t)rows * width;
+      uint32_t dropped = 0;
+      if ((st = mfp_dev_coo_count(rows, rp, width, &dropped, nullptr))) return bail(st);
+      m->width = width;
+      m->nnz = nnz - dropped;
+      m->format_bytes = slots * (vs + 4) + xy_bytes;
+      if ((st = track_bytes(m, &m->vals, slots * vs)) ||
+          (st = track(m, &m->cols_a, slots)) ||
+          (st = mfp_dev_ell_from_csr(vt, rows, rp, ci, data, width, m->vals, m->cols_a, nullptr)))
+        return bail(st);
+      break;
+    }
+    case MFP_FORMAT_COO:
+    case MFP_FORMAT_HYBRID: {
+      const bool hyb = format == MFP_FORMAT_HYBRID;
+      uint32_t cnnz = nnz;
+      if (hyb && (st = mfp_dev_coo_count(rows, rp, width, &cnnz, nullptr))) return bail(st);
+      const uint64_t slots = hyb ? (uint64_t)rows * width : 0u;
+      void **cv = hyb ? &m->vals2 : &m->vals;
+      uint32_t **cc = hyb ? &m->cols2 : &m->cols_a, **cr = hyb ? &m->rows2 : &m->rows_a;
+      if (hyb) {
+        m->width = width;
+        m->coo_nnz = cnnz;
+        if ((st = track_bytes(m, &m->vals, slots * vs)) ||
+            (st = track(m, &m->cols_a, slots)) ||
+            (st = mfp_dev_ell_from_csr(vt, rows, rp, ci, data, width, m->vals, m->cols_a, nullptr)))
+          return bail(st);
+      }
+      m->format_bytes = slots * (vs + 4) + (uint64_t)cnnz * (vs + 8) + xy_bytes;
+      m->ws_bytes = coo_ws_bytes(cnnz);
+      unsigned char *ws = nullptr;
+      if ((st = track_bytes(m, cv, (size_t)cnnz * vs)) || (st = track(m, cc, cnnz)) ||
+          (st = track(m, cr, cnnz)) || (st = track(m, &ws, m->ws_bytes)) ||
+          (st = mfp_dev_coo_from_csr(vt, rows, rp, ci, data, hyb ? width : 0u, *cv, *cc, *cr, nullptr)))
+        return bail(st);
+      m->ws = ws;
+      if (ws && cudaMemset(ws, 0, m->ws_bytes) != cudaSuccess) return bail(fail(MFP_ERROR_CUDA, "cudaMemset workspace"));
+      break;
+    }
+    case MFP_FORMAT_SCOO: {
+      mfp_scoo_params prm{};
+      if (o.scoo) {
+        prm = *o.scoo;
+      } else {
+        mfp_device_info di{};
+        if ((st = mfp_get_device_info(m->device, &di)) ||
+            (st = mfp_scoo_params_compute(rows, di.sm_count, di.shared_mem_per_block, vt, &prm)))
+          return bail(st);
+      }
+      if ((uint64_t)prm.slice_size * prm.slices_count < rows)
+        return bail(fail(MFP_ERROR_INVALID_VALUE, "slices do not cover the rows"));
+      m->slices = prm.slices_count;
+      m->slice_size = prm.slice_size;
+      m->format_bytes = (uint64_t)nnz * (vs + 8) + ((uint64_t)m->slices + 1) * 4 + xy_bytes;
+      uint32_t *dwin = nullptr;
+      if ((st = track_bytes(m, &m->vals, (size_t)nnz * vs)) ||
+          (st = track(m, &m->cols_a, nnz)) || (st = track(m, &m->rows_a, nnz)) ||
+          (st = track(m, &m->aux, (size_t)m->slices + 1)) || (st = dmalloc(&dwin, 2 * (size_t)m->slices)))
+        return bail(st);
+      std::vector<uint32_t> win(2 * (size_t)m->slices), hsp((size_t)m->slices + 1);
+      st = mfp_dev_scoo_from_csr(vt, rows, nnz, rp, ci, data, &prm, m->vals, m->cols_a, m->rows_a, m->aux, nullptr);
+      if (!st) st = mfp_dev_scoo_x_windows(nnz, m->cols_a, m->aux, m->slices, dwin, nullptr);
+      if (!st && (cudaMemcpy(win.data(), dwin, win.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                  cudaMemcpy(hsp.data(), m->aux, hsp.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess))
+        st = fail(MFP_ERROR_CUDA, "cudaMemcpy SCOO metadata");
+      cudaFree(dwin);
+      if (st || (st = scoo_attach_windows(m, win, hsp.data()))) return bail(st);
+      break;
+    }
+    default:
+      return bail(fail(MFP_ERROR_INVALID_VALUE, "bad format"));
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(MFP_ERROR_CUDA, "device conversion"));
   return finish_matrix(m, out);
 }
 

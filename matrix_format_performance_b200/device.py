@@ -141,6 +141,28 @@ class DeviceMatrix:
             return cls.from_hybrid(hm)
         raise ValueError(f"unknown format {fmt}")
 
+    @classmethod
+    def from_device_csr(cls, row_ptr, columns, data, cols: int, fmt: int, *, config: dict | None = None,
+                        ell_width: int | None = None, scoo: "_capi.ScooParams | None" = None) -> "DeviceMatrix":
+        """Builds format `fmt` from a CSR already on the GPU (torch tensors):
+        the layout is converted by the engine's kernels (mfp_matrix_create_device).
+        ell_width: ELL / hybrid ELL part (None = longest row)."""
+        o = _capi.DeviceBuildOptions()
+        o.ell_width = _capi.ELL_WIDTH_LONGEST if ell_width is None else int(ell_width)
+        cfg = _capi.CsrConfig()
+        if config:
+            for k, v in config.items():
+                setattr(cfg, k, int(v))
+            o.csr = C.pointer(cfg)
+        if scoo is not None:
+            o.scoo = C.pointer(scoo)
+        dt = np.dtype(str(data.dtype).replace("torch.", ""))
+        nnz = columns.numel()
+        h = C.c_void_p()
+        call("mfp_matrix_create_device", fmt, _VT[dt], row_ptr.numel() - 1, cols, nnz, _dptr(row_ptr),
+             _dptr(columns) if nnz else None, _dptr(data) if nnz else None, C.byref(o), C.byref(h))
+        return cls(h, fmt, dt)
+
     # -- use ------------------------------------------------------------------
     def info(self) -> _capi.MatrixInfo:
         i = _capi.MatrixInfo()
