@@ -243,36 +243,43 @@ int exclusive_scan(uint32_t n, F f, uint32_t *out, scratch &sc) {
 
 // ---------------------------------------------------------------------------
 // Row expansion: output element j in [0, total) belongs to the row r with
-// tp[r] <= j < tp[r+1]; it copies source element rp[r] + start + (j - tp[r]).
-// With tp == rp and start == 0 this is the plain COO / SCOO copy.
+// tp[r] <= j < tp[r+1] and copies source element rp[r] + start + (j - tp[r]).
+// With tp == rp and start == 0 (plain COO / SCOO) the values and columns are
+// the CSR arrays themselves, copied whole; only the row ids are written here.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(kThreads) expand_kernel(uint32_t rows, uint32_t total, const uint32_t *tp,
+// tr[i] = the row holding output position i * kTile (i < ntiles) or total - 1
+// (i = ntiles): the largest r < rows with tp[r] <= pos.
+__global__ void __launch_bounds__(kThreads) tile_rows_kernel(uint32_t rows, uint32_t total, const uint32_t *tp,
+                                                             uint32_t ntiles, uint32_t *tr) {
+  const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+  if (i > ntiles) return;
+  const uint32_t pos = i < ntiles ? i * kTile : total - 1u;
+  uint32_t lo = 0, hi = rows - 1;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    if (tp[mid] <= pos) lo = mid; else hi = mid - 1;
+  }
+  tr[i] = lo;
+}
+
+template <typename T, bool COPY>
+__global__ void __launch_bounds__(kThreads) expand_kernel(uint32_t total, const uint32_t *tr, const uint32_t *tp,
                                                           const uint32_t *rp, uint32_t start,
                                                           const uint32_t *__restrict__ cols,
                                                           const T *__restrict__ vals, T *__restrict__ od,
                                                           uint32_t *__restrict__ oc, uint32_t *__restrict__ orow) {
   __shared__ uint32_t s_row[kTile + kTile / 32];
   __shared__ uint32_t s[kWarps];
-  __shared__ uint32_t s_r[2];
   const uint32_t j0 = blockIdx.x * kTile;
   const uint32_t n = min(kTile, total - j0);
-  if (threadIdx.x < 2) {
-    // the row holding position pos: the largest r < rows with tp[r] <= pos
-    const uint32_t pos = j0 + (threadIdx.x ? n - 1 : 0u);
-    uint32_t lo = 0, hi = rows - 1;
-    while (lo < hi) {
-      const uint32_t mid = lo + (hi - lo + 1) / 2;
-      if (tp[mid] <= pos) lo = mid; else hi = mid - 1;
-    }
-    s_r[threadIdx.x] = lo;
-  }
+  const uint32_t r0 = tr[blockIdx.x], r1 = tr[blockIdx.x + 1];
   for (uint32_t p = threadIdx.x; p < kTile; p += kThreads) s_row[pad(p)] = 0u;
   __syncthreads();
-  const uint32_t r0 = s_r[0], r1 = s_r[1];
+  // mark the first position of every row starting in this tile (r0 covers
+  // position 0; rows up to r1 may start in the next tile and are skipped)
   for (uint32_t r = r0 + threadIdx.x; r <= r1 && r >= r0; r += kThreads) {
     const uint32_t b = tp[r], e = tp[r + 1];
-    if (b < e) s_row[pad(max(b, j0) - j0)] = r;
+    if (b < e && b < j0 + n) s_row[pad(max(b, j0) - j0)] = r;
   }
   __syncthreads();
   // inclusive max-scan over the tile: each position takes the last row mark
@@ -286,14 +293,45 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(uint32_t rows, uint32_
 #pragma unroll
   for (uint32_t k = 0; k < kItems; ++k) s_row[pad(threadIdx.x * kItems + k)] = max(before, v[k]);
   __syncthreads();
-  for (uint32_t p = threadIdx.x; p < n; p += kThreads) {
-    const uint32_t r = s_row[pad(p)];
-    const uint32_t j = j0 + p;
-    const uint32_t src = rp[r] + start + (j - tp[r]);
-    orow[j] = r;
-    oc[j] = cols[src];
-    od[j] = vals[src];
+  // all loads of a thread are issued before its stores
+  uint32_t src[kItems];
+#pragma unroll
+  for (uint32_t k = 0; k < kItems; ++k) {
+    const uint32_t p = k * kThreads + threadIdx.x;
+    v[k] = p < n ? s_row[pad(p)] : 0u;
+    if (COPY) src[k] = p < n ? rp[v[k]] + start + (j0 + p - tp[v[k]]) : 0u;
   }
+  if (COPY) {
+    T dv[kItems];
+    uint32_t dc[kItems];
+#pragma unroll
+    for (uint32_t k = 0; k < kItems; ++k)
+      if (k * kThreads + threadIdx.x < n) {
+        dv[k] = vals[src[k]];
+        dc[k] = cols[src[k]];
+      }
+#pragma unroll
+    for (uint32_t k = 0; k < kItems; ++k)
+      if (k * kThreads + threadIdx.x < n) {
+        od[j0 + k * kThreads + threadIdx.x] = dv[k];
+        oc[j0 + k * kThreads + threadIdx.x] = dc[k];
+      }
+  }
+#pragma unroll
+  for (uint32_t k = 0; k < kItems; ++k) {
+    const uint32_t p = k * kThreads + threadIdx.x;
+    if (p < n) orow[j0 + p] = v[k];
+  }
+}
+
+// ELL: thread per row, slots in order, column-major stores (coalesced across
+// the warp).  When a CTA's CSR segment fits kEllCap elements and is not much
+// longer than the slots it fills, it is first staged in shared memory with
+// coalesced loads (one pad word per 32: conflict-free for rows of 32).
+constexpr uint32_t kEllCap = 8192;
+template <typename T>
+constexpr size_t ell_smem_bytes() {
+  return (size_t)(kEllCap + kEllCap / 32) * (sizeof(T) + sizeof(uint32_t));
 }
 
 template <typename T>
@@ -301,15 +339,47 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(uint32_t rows, uint32_t w
                                                        const uint32_t *__restrict__ cols,
                                                        const T *__restrict__ vals, T *__restrict__ ed,
                                                        uint32_t *__restrict__ ec) {
-  const uint32_t r = blockIdx.x * kThreads + threadIdx.x;
-  if (r >= rows) return;
-  const uint32_t b = rp[r];
-  const uint32_t len = min(rp[r + 1] - b, width);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sv = reinterpret_cast<T *>(smem_raw);
+  uint32_t *sc = reinterpret_cast<uint32_t *>(sv + kEllCap + kEllCap / 32);
+  const uint32_t r0 = blockIdx.x * kThreads;
+  const uint32_t nr = min(kThreads, rows - r0);
+  const uint32_t seg0 = rp[r0], seg1 = rp[r0 + nr];
+  const uint32_t r = r0 + threadIdx.x;
+  const bool has = r < rows;
+  const uint32_t b = has ? rp[r] : 0u;
+  const uint32_t len = has ? min(rp[r + 1] - b, width) : 0u;
+  const bool staged = seg1 - seg0 <= kEllCap && (uint64_t)(seg1 - seg0) <= 2ull * nr * width;
+  if (staged) {
+    // 8 loads in flight per thread before their shared-memory stores
+    for (uint32_t e0 = seg0 + threadIdx.x; e0 < seg1; e0 += 8u * kThreads) {
+      T vv[8];
+      uint32_t cc[8];
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t e = e0 + k * kThreads;
+        if (e < seg1) {
+          vv[k] = vals[e];
+          cc[k] = cols[e];
+        }
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t e = e0 + k * kThreads;
+        if (e < seg1) {
+          sv[pad(e - seg0)] = vv[k];
+          sc[pad(e - seg0)] = cc[k];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!has) return;
   for (uint32_t s = 0; s < width; ++s) {
     const size_t o = (size_t)s * rows + r;
     if (s < len) {
-      ed[o] = vals[b + s];
-      ec[o] = cols[b + s];
+      ed[o] = staged ? sv[pad(b - seg0 + s)] : vals[b + s];
+      ec[o] = staged ? sc[pad(b - seg0 + s)] : cols[b + s];
     } else {
       ed[o] = T(0);
       ec[o] = 0u;
@@ -619,7 +689,17 @@ int coo_from_csr_t(uint32_t rows, const uint32_t *rp, const uint32_t *ci, const 
   CV_TRY(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   if (total == 0) return ok();
   if (!od || !oc || !orow) return fail(MFP_ERROR_INVALID_VALUE, "null output array");
-  expand_kernel<T><<<blocks_for(total, kTile), kThreads, 0, st>>>(rows, total, tp, rp, start, ci, vals, od, oc, orow);
+  const uint32_t ntiles = blocks_for(total, kTile);
+  uint32_t *tr = nullptr;
+  if ((s = sc.get(&tr, (size_t)ntiles + 1))) return s;
+  tile_rows_kernel<<<blocks_for((uint64_t)ntiles + 1, kThreads), kThreads, 0, st>>>(rows, total, tp, ntiles, tr);
+  if (start) {
+    expand_kernel<T, true><<<ntiles, kThreads, 0, st>>>(total, tr, tp, rp, start, ci, vals, od, oc, orow);
+  } else {
+    CV_TRY(cudaMemcpyAsync(od, vals, (size_t)total * sizeof(T), cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+    CV_TRY(cudaMemcpyAsync(oc, ci, (size_t)total * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+    expand_kernel<T, false><<<ntiles, kThreads, 0, st>>>(total, tr, tp, rp, 0u, ci, vals, od, oc, orow);
+  }
   CV_TRY(cudaGetLastError(), "expand_kernel");
   return ok();
 }
@@ -786,12 +866,19 @@ int mfp_dev_ell_from_csr(int vt, uint32_t rows, const uint32_t *rp, const uint32
   if (!rp || ((uint64_t)rows * width && (!ed || !ec))) return fail(MFP_ERROR_INVALID_VALUE, "null array");
   if (rows == 0 || width == 0) return ok();
   cudaStream_t st = as_stream(stream);
-  if (vt == MFP_F64)
-    ell_kernel<double><<<blocks_for(rows, kThreads), kThreads, 0, st>>>(
+  if (vt == MFP_F64) {
+    CV_TRY(cudaFuncSetAttribute(ell_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ell_smem_bytes<double>()),
+           "cudaFuncSetAttribute");
+    ell_kernel<double><<<blocks_for(rows, kThreads), kThreads, ell_smem_bytes<double>(), st>>>(
         rows, width, rp, ci, static_cast<const double *>(vals), static_cast<double *>(ed), ec);
-  else
-    ell_kernel<float><<<blocks_for(rows, kThreads), kThreads, 0, st>>>(
+  } else {
+    CV_TRY(cudaFuncSetAttribute(ell_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ell_smem_bytes<float>()),
+           "cudaFuncSetAttribute");
+    ell_kernel<float><<<blocks_for(rows, kThreads), kThreads, ell_smem_bytes<float>(), st>>>(
         rows, width, rp, ci, static_cast<const float *>(vals), static_cast<float *>(ed), ec);
+  }
   CV_TRY(cudaGetLastError(), "ell_kernel");
   return ok();
 }
