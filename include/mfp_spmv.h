@@ -249,10 +249,11 @@ int mfp_ell_spmv_f64(uint32_t rows, uint32_t cols, uint32_t width, const double 
 
 /* COO — counterpart of gpu_coo_spmv (gpu_matrix_multiplier.cu:622-716).
  * Rows must be sorted (the coo_matrix_class layout).  A segmented reduction
- * replaces the per-element atomics: rows shared by two tiles are combined
- * through `workspace` (device memory of mfp_coo_workspace_bytes bytes,
- * zero-filled once before its first use; every call leaves it zeroed again).
- * Calls that share a workspace must not overlap on the GPU. */
+ * replaces the per-element atomics, in two launches: each warp reduces 256
+ * elements and writes the rows inside them; a fix-up pass adds up the rows
+ * that cross those tiles, from partial sums kept in `workspace` (device memory
+ * of mfp_coo_workspace_bytes bytes; no initialisation needed).  Results are
+ * deterministic.  Calls that share a workspace must not overlap on the GPU. */
 int mfp_coo_workspace_bytes(uint32_t rows, uint32_t nnz, size_t *bytes);
 int mfp_coo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
                      const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
@@ -260,16 +261,20 @@ int mfp_coo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t nnz, const float *da
 int mfp_coo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t nnz, const double *data,
                      const uint32_t *col_ids, const uint32_t *row_ids, const double *x, double *y,
                      void *workspace, size_t workspace_bytes, void *stream);
-/* Reads the workspace's error word (non-zero: a bounded wait gave up). Synchronous. */
+/* Reads a COO workspace's error word (non-zero: a bounded wait gave up; the
+ * two-pass COO never waits and leaves it 0). Synchronous. */
 int mfp_workspace_error(const void *workspace, uint32_t *error);
 
 /* COO SpMV (float) that allocates nothing.  No counterpart in the reference:
  * it serves callers that may not allocate device memory themselves (hosts
  * that own every byte through their own pool or budget, or loops that cannot
  * take cudaMalloc's latency and implicit synchronisation).  Same arguments and
- * result as mfp_coo_spmv_f32 without the workspace: the look-back scratch is a
- * fixed 1 MiB array inside the library, present on every device that loads
- * it, so nnz is limited to 134,215,680 (larger -> MFP_ERROR_TOO_LARGE).
+ * result as mfp_coo_spmv_f32 without the workspace, within the COO tolerance:
+ * it runs the single-pass COO kernel (2048-element tiles; a tile that ends a
+ * row begun in earlier tiles waits, bounded, for their published partial
+ * sums), whose look-back scratch is a fixed 1 MiB array inside the library,
+ * present on every device that loads it, so nnz is limited to 134,215,680
+ * (larger -> MFP_ERROR_TOO_LARGE).
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call clears the part of the array it uses with cudaMemsetAsync on

@@ -568,7 +568,16 @@ int fill(uint64_t n, T *v, T value, void *stream) {
   return check_launch("fill_kernel launch");
 }
 
+// COO workspace: a 16-byte header (its error word stays 0: the two-pass COO
+// has no waits) and, per 256-element warp tile, the head and tail partial
+// sums (8 bytes each, FP64-sized), the flags and the tail row.
 size_t coo_ws_bytes(uint32_t nnz) {
+  const uint64_t wt = (nnz + (uint64_t)d::kWarpTile - 1) / d::kWarpTile;
+  return sizeof(d::coo_ws_header) + wt * 24u;
+}
+// The single-pass look-back COO (the allocation-free entry point): a header and
+// one tile state per 2048 elements.
+size_t coo_lookback_ws_bytes(uint32_t nnz) {
   const uint64_t tiles = (nnz + (uint64_t)d::kChunk - 1) / d::kChunk;
   return sizeof(d::coo_ws_header) + tiles * sizeof(d::coo_tile_state<double>);
 }
@@ -583,15 +592,51 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   if (!ws || ws_bytes < coo_ws_bytes(nnz))
     return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_ws_bytes(nnz), ws_bytes);
   if (!aligned16(ws)) return fail(MFP_ERROR_INVALID_VALUE, "COO workspace must be 16-byte aligned");
+  const uint32_t n_wt = ceil_div(nnz, d::kWarpTile);
+  unsigned char *base = static_cast<unsigned char *>(ws) + sizeof(d::coo_ws_header);
+  d::coo_carry<T> cw;
+  cw.head = reinterpret_cast<T *>(base);
+  cw.tail = reinterpret_cast<T *>(base + (size_t)n_wt * 8u);
+  cw.flags = reinterpret_cast<uint32_t *>(base + (size_t)n_wt * 16u);
+  cw.tail_row = cw.flags + n_wt;
+  const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
+  const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
+  cudaStream_t s = as_stream(stream);
+  if (vec)
+    d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+  else
+    d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+  int st = check_launch("coo_warp_kernel launch");
+  if (st) return st;
+  if (n_wt > 1) {
+    d::coo_fixup_kernel<T, ACCUM><<<ceil_div(n_wt, d::kBlock), d::kBlock, 0, s>>>(n_wt, cw, y);
+    st = check_launch("coo_fixup_kernel launch");
+  }
+  return st;
+}
+
+// Single pass: 2048-element tiles taken by ticket; a tile that ends a row
+// begun in earlier tiles waits (bounded) for their published partial sums.
+template <typename T>
+int coo_lookback_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
+                      const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
+  if (rows == 0) return ok();
+  if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
+  if (nnz == 0) return fill<T>(rows, y, T(0), stream);
+  if (!data || !cols || !rids || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  if (!ws || ws_bytes < coo_lookback_ws_bytes(nnz))
+    return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_lookback_ws_bytes(nnz),
+                ws_bytes);
+  if (!aligned16(ws)) return fail(MFP_ERROR_INVALID_VALUE, "COO workspace must be 16-byte aligned");
   auto *hdr = reinterpret_cast<d::coo_ws_header *>(ws);
   auto *tiles = reinterpret_cast<d::coo_tile_state<T> *>(hdr + 1);
   const uint32_t grid = ceil_div(nnz, d::kChunk);
   const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
   cudaStream_t s = as_stream(stream);
   if (vec)
-    d::coo_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+    d::coo_kernel<T, true, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
   else
-    d::coo_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
+    d::coo_kernel<T, false, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
   return check_launch("coo_kernel launch");
 }
 
@@ -1398,7 +1443,14 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
     out->algorithmic_bytes = m->nnz * 6 + (uint64_t)m->rows * 4 + ((uint64_t)m->rows + 1) * 4 +
                              (uint64_t)m->cols * 4 + (uint64_t)m->rows * 4;
   out->device_bytes = m->device_bytes;
-  out->kernel_launches = (m->format == MFP_FORMAT_HYBRID && m->coo_nnz) ? 2 : 1;
+  // the two-pass COO launches its fix-up pass when there is more than one warp tile
+  auto coo_launches = [](uint64_t n) -> uint32_t { return n > d::kWarpTile ? 2u : 1u; };
+  if (m->format == MFP_FORMAT_COO)
+    out->kernel_launches = coo_launches(m->nnz);
+  else if (m->format == MFP_FORMAT_HYBRID)
+    out->kernel_launches = 1u + (m->coo_nnz ? coo_launches(m->coo_nnz) : 0u);
+  else
+    out->kernel_launches = 1u;
   return ok();
 }
 
@@ -1871,7 +1923,7 @@ int noalloc_scratch(void **out) {
 extern "C" int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
                                         const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
                                         void *stream) {
-  const size_t need = coo_ws_bytes(nnz);
+  const size_t need = coo_lookback_ws_bytes(nnz);
   if (need > kNoAllocScratchBytes)
     return fail(MFP_ERROR_TOO_LARGE,
                 "nnz %u needs %zu bytes of COO scratch; the fixed scratch holds %zu bytes (nnz <= %zu)", nnz, need,
@@ -1882,5 +1934,5 @@ extern "C" int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t n
   if (st) return st;
   // the workspace must start zeroed; the previous call's contents are cleared on this stream
   if (rows && nnz) CUDA_TRY(cudaMemsetAsync(ws, 0, need, as_stream(stream)), "cudaMemsetAsync(scratch)");
-  return coo_spmv<float>(rows, nnz, data, col_ids, row_ids, x, y, ws, need, stream);
+  return coo_lookback_spmv<float>(rows, nnz, data, col_ids, row_ids, x, y, ws, need, stream);
 }

@@ -412,7 +412,7 @@ int mfp_lowp_deltas(uint32_t nnz, const uint32_t *c, uint16_t *delta, uint32_t *
 int mfp_lowp_ell_from_csr(int vt, int index16, uint32_t rows, uint32_t cols, const uint32_t *rp, const uint32_t *ci,
                           const double *v, uint32_t width, uint16_t *q, void *idx, float *scale) {
   if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
-  if (!rp || !scale || ((uint64_t)width * rows && (!q || !idx))) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  if (!rp || !scale || ((uint64_t)width * rows != 0 && (!q || !idx))) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   const uint32_t nnz = rp[rows];
   if (nnz && (!ci || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   for (uint32_t r = 0; r < rows; ++r)

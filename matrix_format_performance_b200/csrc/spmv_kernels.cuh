@@ -1006,18 +1006,15 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
       if (first_prev && last_next) {
         tiles[tile].value = v;
         tiles[tile].kind = 2u;
-        __threadfence();
         store_release(&tiles[tile].flag, 1u);
       } else if (!first_prev && last_next) {
         tiles[tile].value = v;
         tiles[tile].kind = 1u;
-        __threadfence();
         store_release(&tiles[tile].flag, 1u);
       }
     } else if (last_next) {
       tiles[tile].value = sm.last_total;
       tiles[tile].kind = 1u;
-      __threadfence();
       store_release(&tiles[tile].flag, 1u);
     }
     if (first_prev && !(rf == rl && last_next)) {
@@ -1040,13 +1037,186 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
       if (!ok) atomicOr(&ws->error, 1u);
       if (rf < n_rows) y[rf] = ACCUM ? add_rn(y[rf], add_rn(sum, sm.first_total)) : add_rn(sum, sm.first_total);
     }
-    __threadfence();
+    // the tile state this thread wrote is ordered by the release stores; the
+    // counters are reset by the last CTA and read again only by the next launch
     const uint32_t d = atomicAdd(&ws->done, 1u);
     if (d == gridDim.x - 1) {
       ws->ticket = 0u;
       ws->done = 0u;
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// COO in two passes (the default COO and hybrid-tail path).
+// Pass 1, coo_warp_kernel: warp w reduces the 256 elements [256 w, 256 w + 256):
+// lane l loads elements 8 l .. 8 l + 7 (16-byte loads) and sums its runs of
+// equal rows in order; a segmented scan over the lanes (shuffles) carries the
+// runs that cross lanes.  Rows that start and end inside the warp tile are
+// written to y; the tile's head row (continuing from the previous tile) and
+// tail row (continuing into the next) leave partial sums and flags in the
+// workspace.  Pass 2, coo_fixup_kernel: one thread per warp tile finishes the
+// row that starts in its tile and continues past it, adding the partials of
+// the following tiles in tile order.  No block barriers and no waits between
+// CTAs; every row is summed in a fixed order, so results repeat bit for bit.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kWarpTile = 32u * kEpt;
+constexpr uint32_t kHeadCont = 1u, kTailCont = 2u, kOneRow = 4u;
+
+template <typename T>
+struct coo_carry {
+  T *head, *tail;
+  uint32_t *flags, *tail_row;
+};
+
+// segmented-scan state: the row of the last run of the covered lanes, its sum
+// over those lanes, and whether that row's run starts inside them
+template <typename T>
+struct seg_state {
+  uint32_t row;
+  T val;
+  bool closed;
+};
+template <typename T>
+__device__ __forceinline__ seg_state<T> seg_combine(const seg_state<T> &a, const seg_state<T> &b) {
+  if (b.closed) return b;
+  if (a.row != b.row) return {b.row, b.val, true};
+  return {b.row, add_rn(a.val, b.val), a.closed};
+}
+
+template <typename T, bool ACCUM>
+__device__ __forceinline__ void coo_put(T *y, uint32_t row, T v) {
+  y[row] = ACCUM ? add_rn(y[row], v) : v;
+}
+
+template <typename T, bool VEC, bool ACCUM>
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4)
+    coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                    const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
+                    coo_carry<T> cw) {
+  const uint64_t pol = policy_evict_first();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wt = blockIdx.x * (kBlock / 32u) + (threadIdx.x >> 5);
+  if ((uint64_t)wt * kWarpTile >= nnz) return;  // whole warps only
+  const uint32_t c0 = wt * kWarpTile, c1 = min(nnz, c0 + kWarpTile);
+  T pr[kEpt];
+  uint32_t rw[kEpt], i0 = 0;
+  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + lane * kEpt, c0, c1, pr, rw,
+                                              i0, pol);
+  const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
+  const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
+  const bool active = cnt > 0;
+  const uint32_t last_lane = (c1 - c0 - 1u) / kEpt;
+  // runs inside the lane: the first and last run's sums; middle runs are whole rows
+  uint32_t rf = kNoRow, rl = kNoRow;
+  T sf = T(0), sl = T(0);
+  if (active) {
+    rf = rw[0];
+    rl = rw[cnt - 1u];
+    uint32_t cur = rf;
+    T acc = pr[0];
+    bool first = true;
+#pragma unroll
+    for (uint32_t k = 1; k < kEpt; ++k) {
+      if (k < cnt) {
+        if (rw[k] == cur) {
+          acc = add_rn(acc, pr[k]);
+        } else {
+          if (first) sf = acc;
+          else coo_put<T, ACCUM>(y, cur, acc);
+          if (!ACCUM)
+            for (uint32_t r = cur + 1u; r < rw[k]; ++r) y[r] = T(0);
+          first = false;
+          cur = rw[k];
+          acc = pr[k];
+        }
+      }
+    }
+    if (first) sf = acc;
+    sl = acc;
+  }
+  const bool single = active && rf == rl;
+  // segmented inclusive scan of the lanes' last runs
+  seg_state<T> st{active ? rl : kNoRow, single ? sf : sl, !single};
+  if (!active) st = {kNoRow, T(0), true};
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    seg_state<T> a;
+    a.row = __shfl_up_sync(0xffffffffu, st.row, o);
+    a.val = __shfl_up_sync(0xffffffffu, st.val, o);
+    a.closed = __shfl_up_sync(0xffffffffu, (uint32_t)st.closed, o) != 0u;
+    if (lane >= o) st = seg_combine(a, st);
+  }
+  // carry into this lane: the scan over lanes [0, lane)
+  seg_state<T> cin;
+  cin.row = __shfl_up_sync(0xffffffffu, st.row, 1);
+  cin.val = __shfl_up_sync(0xffffffffu, st.val, 1);
+  cin.closed = __shfl_up_sync(0xffffffffu, (uint32_t)st.closed, 1) != 0u;
+  const uint32_t prev_last = __shfl_up_sync(0xffffffffu, rl, 1);
+  const uint32_t next_first = __shfl_down_sync(0xffffffffu, rf, 1);
+  const uint32_t tile_first = __shfl_sync(0xffffffffu, rf, 0);  // lane 0 is always active
+  if (!active) return;
+  if (lane == 0) cin = {kNoRow, T(0), true};
+  // the lane's first run, with the carry of the lanes before it
+  const bool joined = cin.row == rf;
+  const T ftot = joined ? add_rn(cin.val, sf) : sf;
+  // does the first run's row reach back to the tile start and beyond it?
+  const bool from_prev = rf == prv && (lane == 0 || (joined && !cin.closed));
+  // empty rows before this lane's first row
+  if (!ACCUM) {
+    const uint32_t lo = lane == 0 ? (prv == kNoRow ? 0u : prv + 1u) : prev_last + 1u;
+    for (uint32_t r = lo; r < rf; ++r) y[r] = T(0);
+  }
+  const uint32_t after = lane < last_lane ? next_first : nxt;  // row of the element after this lane
+  if (!single) {
+    // first run ends inside the lane
+    if (from_prev) {
+      cw.head[wt] = ftot;
+    } else {
+      coo_put<T, ACCUM>(y, rf, ftot);
+    }
+  }
+  // last run (the first run too when single)
+  const T ltot = single ? ftot : sl;
+  const bool l_from_prev = single && from_prev;
+  if (after != rl) {
+    if (l_from_prev) cw.head[wt] = ltot;
+    else coo_put<T, ACCUM>(y, rl, ltot);
+  } else if (lane == last_lane) {
+    // the tail row continues into the next tile
+    cw.tail[wt] = ltot;
+    cw.tail_row[wt] = rl;
+    if (l_from_prev) cw.head[wt] = ltot;
+  }
+  if (lane == last_lane) {
+    uint32_t f = 0u;
+    if (tile_first == prv) f |= kHeadCont;  // the tile's first row began in an earlier tile
+    if (rl == nxt) f |= kTailCont;          // its last row goes on in the next tile
+    if (tile_first == rl) f |= kOneRow;
+    cw.flags[wt] = f;
+    if (!ACCUM && c1 == nnz)
+      for (uint32_t r = rl + 1u; r < n_rows; ++r) y[r] = T(0);
+  }
+}
+
+// Pass 2: the row starting in tile w that continues past it.
+template <typename T, bool ACCUM>
+__global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, coo_carry<T> cw, T *__restrict__ y) {
+  const uint32_t w = blockIdx.x * kBlock + threadIdx.x;
+  if (w >= n_tiles) return;
+  const uint32_t f = cw.flags[w];
+  if (!(f & kTailCont) || ((f & kOneRow) && (f & kHeadCont))) return;
+  T acc = cw.tail[w];
+  for (uint32_t k = w + 1u; k < n_tiles; ++k) {
+    const uint32_t g = cw.flags[k];
+    if ((g & kOneRow) && (g & kTailCont)) {
+      acc = add_rn(acc, cw.tail[k]);
+      continue;
+    }
+    acc = add_rn(acc, cw.head[k]);
+    break;
+  }
+  coo_put<T, ACCUM>(y, cw.tail_row[w], acc);
 }
 
 // ---------------------------------------------------------------------------
