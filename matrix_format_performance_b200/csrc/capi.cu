@@ -274,7 +274,7 @@ void free_stream_plan(stream_plan &sp) {
 
 // Streaming-kernel plans for both value types; variant from config.kernel.
 int build_stream_plans(mfp_csr_plan *plan, const uint32_t *rp) {
-  if (plan->nnz == 0 || plan->cfg.kernel < 2) return MFP_SUCCESS;
+  if (plan->nnz == 0 || (plan->cfg.kernel != 2 && plan->cfg.kernel != 3)) return MFP_SUCCESS;
   int st;
   if ((st = dmalloc(&plan->error, 1, &plan->device_bytes))) return st;
   CUDA_TRY(cudaMemset(plan->error, 0, sizeof(uint32_t)), "cudaMemset error word");
@@ -503,7 +503,7 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
   // the exact-order configuration keeps every row in one thread's sequential
   // sum, which only the row-block kernel does for rows split between CTAs
   const bool exact_order = plan->cfg.long_row_threshold == UINT32_MAX && plan->assist_thr == UINT32_MAX;
-  if (vec && aligned16(rp) && sp.grid && !exact_order && plan->cfg.kernel >= 2) {
+  if (vec && aligned16(rp) && sp.grid && !exact_order && (plan->cfg.kernel == 2 || plan->cfg.kernel == 3)) {
     d::stream_args<T> S{};
     S.n_rows = plan->rows;
     S.nnz = plan->nnz;

@@ -1089,22 +1089,15 @@ __device__ __forceinline__ void coo_put(T *y, uint32_t row, T v) {
   y[row] = ACCUM ? add_rn(y[row], v) : v;
 }
 
-template <typename T, bool VEC, bool ACCUM>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4)
-    coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
-                    const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
-                    coo_carry<T> cw) {
-  const uint64_t pol = policy_evict_first();
+// The reduction of one warp tile [c0, c1) of nnz elements, the lane's cnt
+// products pr and rows rw in hand (rows non-decreasing); prv / nxt are the
+// rows of the elements just before and after the tile (kNoRow at the ends).
+template <typename T, bool ACCUM>
+__device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint32_t c1, uint32_t nnz,
+                                                 uint32_t n_rows, const T (&pr)[kEpt], const uint32_t (&rw)[kEpt],
+                                                 uint32_t cnt, uint32_t prv, uint32_t nxt, T *__restrict__ y,
+                                                 const coo_carry<T> &cw) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t wt = blockIdx.x * (kBlock / 32u) + (threadIdx.x >> 5);
-  if ((uint64_t)wt * kWarpTile >= nnz) return;  // whole warps only
-  const uint32_t c0 = wt * kWarpTile, c1 = min(nnz, c0 + kWarpTile);
-  T pr[kEpt];
-  uint32_t rw[kEpt], i0 = 0;
-  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + lane * kEpt, c0, c1, pr, rw,
-                                              i0, pol);
-  const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
-  const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
   const bool active = cnt > 0;
   const uint32_t last_lane = (c1 - c0 - 1u) / kEpt;
   // runs inside the lane: the first and last run's sums; middle runs are whole rows
@@ -1170,11 +1163,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
   const uint32_t after = lane < last_lane ? next_first : nxt;  // row of the element after this lane
   if (!single) {
     // first run ends inside the lane
-    if (from_prev) {
-      cw.head[wt] = ftot;
-    } else {
-      coo_put<T, ACCUM>(y, rf, ftot);
-    }
+    if (from_prev) cw.head[wt] = ftot;
+    else coo_put<T, ACCUM>(y, rf, ftot);
   }
   // last run (the first run too when single)
   const T ltot = single ? ftot : sl;
@@ -1197,6 +1187,25 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
     if (!ACCUM && c1 == nnz)
       for (uint32_t r = rl + 1u; r < n_rows; ++r) y[r] = T(0);
   }
+}
+
+template <typename T, bool VEC, bool ACCUM>
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4)
+    coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                    const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
+                    coo_carry<T> cw) {
+  const uint64_t pol = policy_evict_first();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wt = blockIdx.x * (kBlock / 32u) + (threadIdx.x >> 5);
+  if ((uint64_t)wt * kWarpTile >= nnz) return;  // whole warps only
+  const uint32_t c0 = wt * kWarpTile, c1 = min(nnz, c0 + kWarpTile);
+  T pr[kEpt];
+  uint32_t rw[kEpt], i0 = 0;
+  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + lane * kEpt, c0, c1, pr, rw,
+                                              i0, pol);
+  const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
+  const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
+  warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw);
 }
 
 // Pass 2: the row starting in tile w that continues past it.
