@@ -1208,24 +1208,47 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
   warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw);
 }
 
-// Pass 2: the row starting in tile w that continues past it.
+// Pass 2: the row starting in tile w that continues past it.  The tiles that
+// follow are read 16 at a time (their loads in flight together) and walked in
+// order in registers: a row of 50,000 elements spans 195 tiles, and one
+// dependent load per tile would make it the launch's critical path.
+#ifndef MFP_FIXUP_BATCH
+#define MFP_FIXUP_BATCH 16
+#endif
 template <typename T, bool ACCUM>
 __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, coo_carry<T> cw, T *__restrict__ y) {
+  constexpr uint32_t B = MFP_FIXUP_BATCH;
   const uint32_t w = blockIdx.x * kBlock + threadIdx.x;
   if (w >= n_tiles) return;
   const uint32_t f = cw.flags[w];
   if (!(f & kTailCont) || ((f & kOneRow) && (f & kHeadCont))) return;
   T acc = cw.tail[w];
-  for (uint32_t k = w + 1u; k < n_tiles; ++k) {
-    const uint32_t g = cw.flags[k];
-    if ((g & kOneRow) && (g & kTailCont)) {
-      acc = add_rn(acc, cw.tail[k]);
-      continue;
+  const uint32_t row = cw.tail_row[w];
+  // the row ends in the first following tile that does not hold only this row
+  // and continue; the last tile never continues, so that tile exists
+  for (uint32_t k0 = w + 1u; k0 < n_tiles; k0 += B) {
+    uint32_t g[B];
+    T t[B];
+#pragma unroll
+    for (uint32_t j = 0; j < B; ++j) {
+      const uint32_t k = k0 + j;
+      g[j] = k < n_tiles ? cw.flags[k] : 0u;
+      t[j] = k < n_tiles ? cw.tail[k] : T(0);
     }
-    acc = add_rn(acc, cw.head[k]);
-    break;
+    uint32_t end = B;
+#pragma unroll
+    for (uint32_t j = 0; j < B; ++j) {
+      if (end == B) {
+        if ((g[j] & kOneRow) && (g[j] & kTailCont)) acc = add_rn(acc, t[j]);
+        else end = j;
+      }
+    }
+    if (end < B) {
+      acc = add_rn(acc, cw.head[k0 + end]);
+      break;
+    }
   }
-  coo_put<T, ACCUM>(y, cw.tail_row[w], acc);
+  coo_put<T, ACCUM>(y, row, acc);
 }
 
 // ---------------------------------------------------------------------------
