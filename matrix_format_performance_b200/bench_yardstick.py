@@ -1,6 +1,7 @@
 """The engine's formats beside cuSPARSE's generic SpMV (the vendor yardstick).
 
     python -m matrix_format_performance_b200.bench_yardstick [--rows 4194304] [--stencil 128] [--banded 8388608]
+        [--which power_law,stencil,banded]
 
 For the power-law, stencil and banded matrices (FP32): median device time of
 the engine's CSR scalar / vector / adaptive, COO, SCOO and hybrid kernels and
@@ -54,15 +55,18 @@ def main() -> None:
     ap.add_argument("--rows", type=int, default=4_194_304)
     ap.add_argument("--stencil", type=int, default=128)
     ap.add_argument("--banded", type=int, default=8_388_608)
+    ap.add_argument("--which", default="power_law,stencil,banded")
     a = ap.parse_args()
     import torch
 
     from . import synth
     torch.cuda.set_device(0)
-    for name, gen in ((f"power_law_{a.rows}", lambda: synth.power_law(rows=a.rows, seed=0, cols=a.rows)),
-                      (f"stencil27_{a.stencil}", lambda: synth.stencil_27(a.stencil)),
-                      (f"banded_{a.banded}", lambda: synth.banded(n=a.banded))):
-        print(json.dumps(measure(name, gen().astype(np.float32))), flush=True)
+    which = set(a.which.split(","))
+    for key, name, gen in (("power_law", f"power_law_{a.rows}", lambda: synth.power_law(rows=a.rows, seed=0, cols=a.rows)),
+                           ("stencil", f"stencil27_{a.stencil}", lambda: synth.stencil_27(a.stencil)),
+                           ("banded", f"banded_{a.banded}", lambda: synth.banded(n=a.banded))):
+        if key in which:
+            print(json.dumps(measure(name, gen().astype(np.float32))), flush=True)
 
 
 if __name__ == "__main__":

@@ -1,7 +1,7 @@
 // Benchmark driver with the reference's command line and result files
 // (main.cpp:82-283 perform_measurement, :395-505 main):
 //
-//     mfp_driver /path/to/mtx_list
+//     mfp_driver [--hybrid-sweep] /path/to/mtx_list
 //
 // For every Matrix Market file named in the list (one path per line), in
 // float and double: CSR conversion, the CPU CSR columns (one single-thread run
@@ -20,6 +20,11 @@
 // layout plus five vectors, as the reference estimates) are skipped, as are
 // ELL layouts more than 64x larger than the CSR layout (the engine measures
 // the other formats of such a matrix rather than dropping it).
+// --hybrid-sweep adds the reference's disabled hybrid sweep (main.cpp:247-279):
+// ELL part from avg + (max - avg) * percent for percent = 0, 0.35, 0.70, both
+// hybrid operators, 20 runs each, keyed "<label> <percent>%" (the reference's
+// per-percent labels are commented out, so its results would collide); a
+// percent whose ELL part is more than 64x the CSR layout is skipped.
 // Clocks are never changed: the reference's application-clock locking is not
 // built.  MKL and cusp columns are not measured.
 #include <cuda_runtime.h>
@@ -81,7 +86,7 @@ std::string file_name(const std::string &path) {
 
 template <typename data_type>
 std::vector<measurement_class> perform_measurement(const matrix_market::reader &reader, size_t free_memory,
-                                                   int sm_count, size_t shared_mem_size) {
+                                                   int sm_count, size_t shared_mem_size, bool hybrid_sweep) {
   std::vector<measurement_class> out;
   csr_matrix_class<data_type> csr(reader.matrix());
   const auto &meta = csr.meta;
@@ -150,16 +155,41 @@ std::vector<measurement_class> perform_measurement(const matrix_market::reader &
                                                reference_answer.get());
     });
   }
+  if (hybrid_sweep) {
+    const auto st = get_rows_statistics(meta, csr.row_ptr.get());
+    hybrid_matrix_class<data_type> hybrid(csr);
+    for (int step = 0; step < 3; ++step) {
+      const double percent = 0.35 * step;  // the reference's loop: 0.0, 0.35, 0.70 (<= 1.0)
+      const unsigned int width = st.avg_elements_in_rows + (st.max_elements_in_rows - st.avg_elements_in_rows) * percent;
+      if ((size_t)width * meta.rows_count * (sizeof(data_type) + 4) > 64 * std::max<size_t>(csr_bytes, 1)) continue;
+      hybrid.allocate(csr, percent);
+      const std::string tag = " " + std::to_string((int)(percent * 100)) + "%";
+      repeat([&](bool) {
+        auto m = gpu_hybrid_spmv<data_type>(hybrid, A, A_coo, col_ids, col_ids_coo, row_ptr, x_gpu, y, x.get(),
+                                            reference_answer.get());
+        m.set_format(m.get_format() + tag);
+        return m;
+      });
+      repeat([&](bool) {
+        auto m = gpu_hybrid_atomic_spmv<data_type>(hybrid, A, A_coo, col_ids, col_ids_coo, row_ptr, x_gpu, y, x.get(),
+                                                   reference_answer.get());
+        m.set_format(m.get_format() + tag);
+        return m;
+      });
+    }
+  }
   return out;
 }
 
 }  // namespace
 
 int main(int argc, char *argv[]) {
-  if (argc != 2) {
-    std::cerr << "Usage: " << argv[0] << " /path/to/mtx_list" << std::endl;
+  const bool hybrid_sweep = argc == 3 && std::string(argv[1]) == "--hybrid-sweep";
+  if (argc != 2 && !hybrid_sweep) {
+    std::cerr << "Usage: " << argv[0] << " [--hybrid-sweep] /path/to/mtx_list" << std::endl;
     return 1;
   }
+  const char *list_path = argv[argc - 1];
   const int gpu_id = 0;
   if (cudaSetDevice(gpu_id) != cudaSuccess) {
     std::cerr << "CUDA device " << gpu_id << " is not available" << std::endl;
@@ -176,9 +206,9 @@ int main(int argc, char *argv[]) {
     return 1;
   }
 
-  std::ifstream list(argv[1]);
+  std::ifstream list(list_path);
   if (!list) {
-    std::cerr << "cannot open " << argv[1] << std::endl;
+    std::cerr << "cannot open " << list_path << std::endl;
     return 1;
   }
   std::map<std::string, table> elapsed, bandwidth, throughput, model_bw, max_error;
@@ -196,8 +226,10 @@ int main(int argc, char *argv[]) {
       std::cout << "Complete loading (rows: " << meta.rows_count << "; cols: " << meta.cols_count
                 << "; nnz: " << meta.non_zero_count << ")" << std::endl;
       std::map<std::string, std::vector<measurement_class>> results;
-      results["float"] = perform_measurement<float>(reader, free_mem, dev.sm_count, dev.shared_mem_per_block);
-      results["double"] = perform_measurement<double>(reader, free_mem, dev.sm_count, dev.shared_mem_per_block);
+      results["float"] =
+          perform_measurement<float>(reader, free_mem, dev.sm_count, dev.shared_mem_per_block, hybrid_sweep);
+      results["double"] =
+          perform_measurement<double>(reader, free_mem, dev.sm_count, dev.shared_mem_per_block, hybrid_sweep);
       const std::string name = file_name(mtx);
       if (results["float"].empty() || results["double"].empty()) continue;  // did not fit on the GPU
       for (auto &[type, res] : results)

@@ -31,6 +31,8 @@ class measurement_class {
   double get_computational_throughput() const { return computational_throughput; }
   double get_model_bandwidth() const { return model_bandwidth_; }
   const std::string &get_format() const { return matrix_format; }
+  // engine extension: relabel a record (the hybrid sweep keys its results by percent)
+  void set_format(std::string f) { matrix_format = std::move(f); }
   // relative squared L2 error of the last compare_results against the reference answer
   double error = 0.0;
 

@@ -16,6 +16,7 @@ import pytest
 
 from conftest import golden_cases, load_golden
 from matrix_format_performance_b200 import build as B
+from matrix_format_performance_b200 import formats as F
 from matrix_format_performance_b200 import synth
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -132,3 +133,34 @@ def test_driver_runs_every_operator(tmp_path):
             assert max(err[name].values()) <= 1e-9, (prec, name, err[name])
         for name, m in mats.items():
             assert info[name]["nnz"] == m.nnz and info[name]["rows"] == m.rows
+
+
+@pytest.mark.gpu
+def test_driver_hybrid_sweep(tmp_path):
+    """--hybrid-sweep: the reference's disabled sweep (percent 0, 0.35, 0.70),
+    keyed by percent; a percent whose ELL part exceeds 64x the CSR layout is
+    skipped (the power-law matrix's 0.70 width)."""
+    drv = B.build_driver()
+    mats = {"banded_20k.mtx": synth.banded(n=20_000, seed=6),
+            "powerlaw_20k.mtx": synth.power_law(rows=20_000, k_hi=2_000, seed=7)}
+    for name, m in mats.items():
+        rows = np.repeat(np.arange(m.rows), np.diff(m.row_ptr.astype(np.int64)))
+        write_mtx(tmp_path / name, m.rows, m.cols, rows, m.columns, m.data)
+    (tmp_path / "list.txt").write_text("\n".join(str(tmp_path / n) for n in mats) + "\n")
+    r = subprocess.run([str(drv), "--hybrid-sweep", str(tmp_path / "list.txt")], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    for prec in ("float", "double"):
+        t = json.loads((tmp_path / f"{prec}.json").read_text())
+        err = json.loads((tmp_path / f"{prec}_max_error.json").read_text())
+        for name, m in mats.items():
+            stats = F.get_rows_statistics(m)
+            csr_bytes = m.nnz * (4 if prec == "float" else 8) + m.nnz * 4
+            for pct in (0, 35, 70):
+                w = int(stats.avg_elements_in_rows + (stats.max_elements_in_rows - stats.avg_elements_in_rows) * pct / 100)
+                fits = w * m.rows * ((4 if prec == "float" else 8) + 4) <= 64 * csr_bytes
+                for label in ("GPU Hybrid (TODO)", "GPU Hybrid (atomic)"):
+                    key = f"{label} {pct}%"
+                    assert (key in t[name]) == fits, (prec, name, key, w)
+                    if fits:
+                        assert t[name][key] > 0 and err[name][key] <= 1e-9
