@@ -1069,21 +1069,6 @@ struct coo_carry {
   uint32_t *flags, *tail_row;
 };
 
-// segmented-scan state: the row of the last run of the covered lanes, its sum
-// over those lanes, and whether that row's run starts inside them
-template <typename T>
-struct seg_state {
-  uint32_t row;
-  T val;
-  bool closed;
-};
-template <typename T>
-__device__ __forceinline__ seg_state<T> seg_combine(const seg_state<T> &a, const seg_state<T> &b) {
-  if (b.closed) return b;
-  if (a.row != b.row) return {b.row, b.val, true};
-  return {b.row, add_rn(a.val, b.val), a.closed};
-}
-
 template <typename T, bool ACCUM>
 __device__ __forceinline__ void coo_put(T *y, uint32_t row, T v) {
   y[row] = ACCUM ? add_rn(y[row], v) : v;
@@ -1129,32 +1114,31 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
     sl = acc;
   }
   const bool single = active && rf == rl;
-  // segmented inclusive scan of the lanes' last runs
-  seg_state<T> st{active ? rl : kNoRow, single ? sf : sl, !single};
-  if (!active) st = {kNoRow, T(0), true};
-#pragma unroll
-  for (uint32_t o = 1; o < 32; o <<= 1) {
-    seg_state<T> a;
-    a.row = __shfl_up_sync(0xffffffffu, st.row, o);
-    a.val = __shfl_up_sync(0xffffffffu, st.val, o);
-    a.closed = __shfl_up_sync(0xffffffffu, (uint32_t)st.closed, o) != 0u;
-    if (lane >= o) st = seg_combine(a, st);
-  }
-  // carry into this lane: the scan over lanes [0, lane)
-  seg_state<T> cin;
-  cin.row = __shfl_up_sync(0xffffffffu, st.row, 1);
-  cin.val = __shfl_up_sync(0xffffffffu, st.val, 1);
-  cin.closed = __shfl_up_sync(0xffffffffu, (uint32_t)st.closed, 1) != 0u;
   const uint32_t prev_last = __shfl_up_sync(0xffffffffu, rl, 1);
   const uint32_t next_first = __shfl_down_sync(0xffffffffu, rf, 1);
   const uint32_t tile_first = __shfl_sync(0xffffffffu, rf, 0);  // lane 0 is always active
+  // the lane's first row continues the previous lane's last row
+  const bool cont = active && lane > 0 && rf == prev_last;
+  // Segmented inclusive scan of the lanes' last-run sums.  A lane closes its
+  // segment unless it holds a single run that continues the previous lane;
+  // rows are sorted, so an unclosed chain of lanes is one row and only the
+  // sums travel by shuffle (the closed state of a window comes from the mask).
+  const uint32_t closed = __ballot_sync(0xffffffffu, !(single && cont));
+  T v = active ? (single ? sf : sl) : T(0);
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const T a = __shfl_up_sync(0xffffffffu, v, o);
+    // this lane's window is lanes (lane - o, lane]; add the window before it
+    // unless a lane of this window closes the segment
+    if (lane >= o && (closed & (((1u << o) - 1u) << (lane + 1u - o))) == 0u) v = add_rn(a, v);
+  }
+  const T cin_val = __shfl_up_sync(0xffffffffu, v, 1);  // lane - 1's chain: the row rf when cont
   if (!active) return;
-  if (lane == 0) cin = {kNoRow, T(0), true};
   // the lane's first run, with the carry of the lanes before it
-  const bool joined = cin.row == rf;
-  const T ftot = joined ? add_rn(cin.val, sf) : sf;
-  // does the first run's row reach back to the tile start and beyond it?
-  const bool from_prev = rf == prv && (lane == 0 || (joined && !cin.closed));
+  const T ftot = cont ? add_rn(cin_val, sf) : sf;
+  // rows are sorted: the first run reaches back beyond the tile exactly when
+  // its row is the row before the tile
+  const bool from_prev = rf == prv;
   // empty rows before this lane's first row
   if (!ACCUM) {
     const uint32_t lo = lane == 0 ? (prv == kNoRow ? 0u : prv + 1u) : prev_last + 1u;
