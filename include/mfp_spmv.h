@@ -142,6 +142,18 @@ int mfp_scoo_from_csr_f64(uint32_t rows, const uint32_t *row_ptr, const uint32_t
                           const double *data, const mfp_scoo_params *params, double *values,
                           uint32_t *c_index, uint32_t *r_index, uint32_t *slices_ptr);
 
+/* The reference's disabled sort_cols option of scoo_matrix_class
+ * (scoo_matrix_class.cpp:102-138): orders each slice's elements by column, in
+ * place, on SCOO arrays built by mfp_scoo_from_csr_*.  The reference sorts with
+ * std::sort (not stable: equal columns in unspecified order); this sort is
+ * stable, so equal columns keep their CSR order.  Rows are then no longer
+ * contiguous within a slice: SpMV goes through mfp_scoo_spmv_unsorted_* (or a
+ * handle, which detects the layout). */
+int mfp_scoo_sort_cols_f32(uint32_t slices_count, const uint32_t *slices_ptr, float *values,
+                           uint32_t *c_index, uint32_t *r_index);
+int mfp_scoo_sort_cols_f64(uint32_t slices_count, const uint32_t *slices_ptr, double *values,
+                           uint32_t *c_index, uint32_t *r_index);
+
 /* fill_row_blocks — gpu/csr_adaptive_spmv.cu:180-240, with NNZ_PER_WG as a
  * parameter (the reference fixes it at 64).  row_blocks may be NULL to count
  * only; otherwise it receives count+1 boundaries. */
@@ -183,6 +195,11 @@ int mfp_dev_scoo_from_csr(int value_type, uint32_t rows, uint32_t nnz, const uin
                           const uint32_t *columns, const void *data, const mfp_scoo_params *params,
                           void *values, uint32_t *c_index, uint32_t *r_index, uint32_t *slices_ptr,
                           void *stream);
+/* mfp_scoo_sort_cols_* on the device (waits): each slice's elements ordered
+ * by column, stably, in place; the slice of an element is r_index / slice_size
+ * (the layout of mfp_dev_scoo_from_csr). */
+int mfp_dev_scoo_sort_cols(int value_type, uint32_t rows, uint32_t cols, uint32_t slice_size, uint32_t nnz,
+                           void *values, uint32_t *c_index, uint32_t *r_index, void *stream);
 /* mfp_scoo_x_windows on the device: [min col, max col + 1) per slice. */
 int mfp_dev_scoo_x_windows(uint32_t nnz, const uint32_t *c_index, const uint32_t *slices_ptr, uint32_t slices,
                            uint32_t *windows, void *stream);
@@ -305,6 +322,18 @@ int mfp_scoo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t slices_count, uint3
                       const double *values, const uint32_t *c_index, const uint32_t *r_index,
                       const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
                       const uint32_t *slice_order, const double *x, double *y, void *stream);
+/* SCOO whose slices are in column order (mfp_scoo_sort_cols_*, the reference's
+ * sort_cols layout): rows within a slice in any order; products are added
+ * into shared-memory row accumulators with atomics, as in the reference
+ * kernel, so the summation order within a row is not fixed.  Same arguments. */
+int mfp_scoo_spmv_unsorted_f32(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
+                               const float *values, const uint32_t *c_index, const uint32_t *r_index,
+                               const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
+                               const uint32_t *slice_order, const float *x, float *y, void *stream);
+int mfp_scoo_spmv_unsorted_f64(uint32_t rows, uint32_t cols, uint32_t slices_count, uint32_t slice_size,
+                               const double *values, const uint32_t *c_index, const uint32_t *r_index,
+                               const uint32_t *slices_ptr, const uint32_t *x_windows, uint32_t max_window,
+                               const uint32_t *slice_order, const double *x, double *y, void *stream);
 
 /* Hybrid ELL + COO — counterpart of gpu_hybrid_spmv / gpu_hybrid_atomic_spmv
  * (gpu_matrix_multiplier.cu:866-1096).  Two launches: the ELL kernel writes
@@ -475,6 +504,9 @@ int mfp_matrix_create_ell(int value_type, uint32_t rows, uint32_t cols, uint32_t
 int mfp_matrix_create_coo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
                           const uint32_t *coo_rows, const uint32_t *coo_cols,
                           const void *coo_data, mfp_matrix **out);
+/* SCOO: rows within each slice may be in CSR order (the reference layout) or
+ * in any order (the sort_cols layout, detected here: SpMV then uses the
+ * shared-memory-atomics kernel). */
 int mfp_matrix_create_scoo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
                            const mfp_scoo_params *params, const uint32_t *c_index,
                            const uint32_t *r_index, const uint32_t *slices_ptr,
@@ -502,6 +534,7 @@ typedef struct mfp_device_build_options {
   const mfp_csr_config *csr;   /* CSR family launch configuration (NULL = defaults) */
   uint32_t ell_width;          /* ELL / hybrid ELL part: slots per row, or MFP_ELL_WIDTH_LONGEST */
   const mfp_scoo_params *scoo; /* SCOO parameters (NULL = mfp_scoo_params_compute for this device) */
+  uint32_t scoo_sort_cols;     /* SCOO: non-zero = each slice in column order (mfp_dev_scoo_sort_cols) */
 } mfp_device_build_options;
 int mfp_matrix_create_device(int format, int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
                              const uint32_t *row_ptr, const uint32_t *columns, const void *data,

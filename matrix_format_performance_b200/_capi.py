@@ -193,7 +193,8 @@ _RESTYPES["mfp_mlp_param_count"] = u32
 
 
 class DeviceBuildOptions(C.Structure):
-    _fields_ = [("csr", C.POINTER(CsrConfig)), ("ell_width", u32), ("scoo", C.POINTER(ScooParams))]
+    _fields_ = [("csr", C.POINTER(CsrConfig)), ("ell_width", u32), ("scoo", C.POINTER(ScooParams)),
+                ("scoo_sort_cols", u32)]
 
 
 ELL_WIDTH_LONGEST = 0xFFFFFFFF
@@ -205,6 +206,11 @@ _PROTOS.update({
     "mfp_dev_ell_from_csr": [i32, u32, vp, vp, vp, u32, vp, vp, vp],
     "mfp_dev_scoo_from_csr": [i32, u32, u32, vp, vp, vp, C.POINTER(ScooParams), vp, vp, vp, vp, vp],
     "mfp_dev_scoo_x_windows": [u32, vp, vp, u32, vp, vp],
+    "mfp_dev_scoo_sort_cols": [i32, u32, u32, u32, u32, vp, vp, vp, vp],
+    "mfp_scoo_sort_cols_f32": [u32, vp, vp, vp, vp],
+    "mfp_scoo_sort_cols_f64": [u32, vp, vp, vp, vp],
+    "mfp_scoo_spmv_unsorted_f32": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp],
+    "mfp_scoo_spmv_unsorted_f64": [u32, u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp],
     "mfp_dev_csr_from_coo": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp],
     "mfp_dev_scratch_bytes": [C.POINTER(u64)],
     "mfp_dev_scratch_release": [],

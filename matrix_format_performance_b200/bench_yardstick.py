@@ -4,7 +4,8 @@
         [--which power_law,stencil,banded]
 
 For the power-law, stencil and banded matrices (FP32): median device time of
-the engine's CSR scalar / vector / adaptive, COO, SCOO and hybrid kernels and
+the engine's CSR scalar / vector / adaptive, COO, SCOO (also with each slice in
+column order, the reference's disabled sort_cols option) and hybrid kernels and
 of cusparseSpMV on CSR (default, ALG1, ALG2) and COO (default), 20 launches
 each with L2 flushed before every launch.  One JSON line per matrix with ms and
 algorithmic GB/s.
@@ -36,6 +37,11 @@ def measure(name, m, reps=20):
         _, med = dm.time(x, y, reps=reps, flush_l2=True)
         out["engine"][LABELS[fmt]] = {"ms": med * 1e3, "gbs": nbytes / med / 1e9}
         dm.close()
+    # SCOO with each slice in column order (the reference's disabled sort_cols option)
+    dm = DeviceMatrix.from_scoo(F.scoo_matrix_class(dev.sm_count, int(dev.shared_mem_per_block), m, sort_cols=True))
+    _, med = dm.time(x, y, reps=reps, flush_l2=True)
+    out["engine"]["GPU SCOO (sorted columns)"] = {"ms": med * 1e3, "gbs": nbytes / med / 1e9}
+    dm.close()
     rp = torch.from_numpy(m.row_ptr.view(np.int32)).cuda()
     ci = torch.from_numpy(m.columns.view(np.int32)).cuda()
     va = torch.from_numpy(m.data).cuda()

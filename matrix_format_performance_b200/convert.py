@@ -81,6 +81,12 @@ def scoo_from_csr(row_ptr, columns, data, params: _capi.ScooParams, stream=None)
     return ov, oc, orow, sp
 
 
+def scoo_sort_cols(values, c_index, r_index, rows: int, cols: int, slice_size: int, stream=None) -> None:
+    """The sort_cols layout (scoo_matrix_class.cpp:102-138, stable) of device SCOO arrays, in place."""
+    call("mfp_dev_scoo_sort_cols", _vt(values), rows, cols, slice_size, values.numel(), _p(values), _p(c_index),
+         _p(r_index), _stream(stream))
+
+
 def hybrid_from_csr(row_ptr, columns, data, width: int, stream=None):
     """hybrid_matrix_class::allocate (matrix_converter.cpp:296-310) at a given
     ELL width -> ((ell_data, ell_columns), (coo_data, coo_cols, coo_rows))."""

@@ -640,11 +640,11 @@ int coo_lookback_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t
   return check_launch("coo_kernel launch");
 }
 
-template <typename T, bool VEC, bool XWIN>
+template <typename T, bool VEC, bool XWIN, bool UNSORTED = false>
 int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32_t slice, const T *v,
                 const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
                 const uint32_t *order, const T *x, T *y) {
-  auto k = d::scoo_kernel<T, VEC, XWIN>;
+  auto k = UNSORTED ? d::scoo_unsorted_kernel<T, XWIN> : d::scoo_kernel<T, VEC, XWIN>;
   if (dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
     const int st = ensure_dyn_smem((const void *)k, dyn, "scoo_kernel");
     if (st) return st;
@@ -656,7 +656,7 @@ int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32
   return ok();
 }
 
-template <typename T>
+template <typename T, bool UNSORTED = false>
 int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const uint32_t *ci,
               const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const uint32_t *order,
               const T *x, T *y, void *stream) {
@@ -671,6 +671,10 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
     return fail(MFP_ERROR_NOT_SUPPORTED, "slice_size %u / window %u too large for shared memory", slice, maxw);
   const bool vec = aligned16(v) && aligned16(ci) && aligned16(ri);
   cudaStream_t s = as_stream(stream);
+  if (UNSORTED) {
+    if (win) return scoo_launch<T, false, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+    return scoo_launch<T, false, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  }
   if (vec) {
     if (win) return scoo_launch<T, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
     return scoo_launch<T, true, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
@@ -868,6 +872,16 @@ int mfp_scoo_spmv_f64(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, 
                       const uint32_t *order, const double *x, double *y, void *s) {
   return scoo_spmv<double>(rows, slices, slice, v, ci, ri, sp, win, maxw, order, x, y, s);
 }
+int mfp_scoo_spmv_unsorted_f32(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, const float *v,
+                               const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win,
+                               uint32_t maxw, const uint32_t *order, const float *x, float *y, void *s) {
+  return scoo_spmv<float, true>(rows, slices, slice, v, ci, ri, sp, win, maxw, order, x, y, s);
+}
+int mfp_scoo_spmv_unsorted_f64(uint32_t rows, uint32_t, uint32_t slices, uint32_t slice, const double *v,
+                               const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win,
+                               uint32_t maxw, const uint32_t *order, const double *x, double *y, void *s) {
+  return scoo_spmv<double, true>(rows, slices, slice, v, ci, ri, sp, win, maxw, order, x, y, s);
+}
 int mfp_lowp_spmv(int vt, uint32_t rows, uint32_t, uint32_t nnz, const uint32_t *rp, const uint16_t *q,
                   const float *scale, const uint32_t *cols, const uint16_t *delta, const uint32_t *base,
                   const float *x, float *y, void *s) {
@@ -939,6 +953,7 @@ struct mfp_matrix {
   float *scale = nullptr;
   uint16_t *delta = nullptr;          // 16-bit column deltas (else cols_a)
   uint32_t *base = nullptr;
+  bool rows_unsorted = false;         // SCOO in the sort_cols layout
 };
 
 namespace {
@@ -1135,6 +1150,7 @@ int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, c
   *out = nullptr;
   if (!valid_vt(vt) || !prm || !sp) return fail(MFP_ERROR_INVALID_VALUE, "bad argument");
   if (nnz && (!ci || !ri || !v)) return fail(MFP_ERROR_INVALID_VALUE, "null host array");
+  bool rows_unsorted = false;
   {
     int st0 = check_columns(ci, nnz, cols);
     if (st0) return st0;
@@ -1145,9 +1161,10 @@ int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, c
       if (b >= e) continue;
       if (e > nnz) return fail(MFP_ERROR_INVALID_VALUE, "slices_ptr[%u] beyond nnz", s + 1);
       const uint64_t r0 = (uint64_t)s * prm->slice_size, r1 = std::min<uint64_t>(rows, r0 + prm->slice_size);
-      for (uint32_t k = b; k < e; ++k)
-        if (ri[k] < r0 || ri[k] >= r1 || (k > b && ri[k] < ri[k - 1]))
-          return fail(MFP_ERROR_INVALID_VALUE, "r_index[%u] outside slice %u or unsorted", k, s);
+      for (uint32_t k = b; k < e; ++k) {
+        if (ri[k] < r0 || ri[k] >= r1) return fail(MFP_ERROR_INVALID_VALUE, "r_index[%u] outside slice %u", k, s);
+        if (k > b && ri[k] < ri[k - 1]) rows_unsorted = true;  // the sort_cols layout
+      }
     }
   }
   const size_t vs = value_size(vt);
@@ -1160,6 +1177,7 @@ int mfp_matrix_create_scoo(int vt, uint32_t rows, uint32_t cols, uint32_t nnz, c
   m->nnz = nnz;
   m->slices = prm->slices_count;
   m->slice_size = prm->slice_size;
+  m->rows_unsorted = rows_unsorted;
   m->format_bytes = (uint64_t)nnz * (vs + 8) + ((uint64_t)m->slices + 1) * 4 + (uint64_t)cols * vs + (uint64_t)rows * vs;
   std::vector<uint32_t> win(2 * (size_t)m->slices);
   mfp_scoo_x_windows(nnz, ci, sp, m->slices, win.data());
@@ -1235,7 +1253,8 @@ int mfp_matrix_create_device(int format, int vt, uint32_t rows, uint32_t cols, u
   if (nnz && (!ci || !data)) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   int st = mfp_dev_check_csr(rows, cols, nnz, rp, ci, nullptr);
   if (st) return st;
-  const mfp_device_build_options o = opt ? *opt : mfp_device_build_options{nullptr, MFP_ELL_WIDTH_LONGEST, nullptr};
+  const mfp_device_build_options o =
+      opt ? *opt : mfp_device_build_options{nullptr, MFP_ELL_WIDTH_LONGEST, nullptr, 0u};
   const size_t vs = value_size(vt);
   auto *m = new mfp_matrix();
   cudaGetDevice(&m->device);
@@ -1335,6 +1354,10 @@ int mfp_matrix_create_device(int format, int vt, uint32_t rows, uint32_t cols, u
         return bail(st);
       std::vector<uint32_t> win(2 * (size_t)m->slices), hsp((size_t)m->slices + 1);
       st = mfp_dev_scoo_from_csr(vt, rows, nnz, rp, ci, data, &prm, m->vals, m->cols_a, m->rows_a, m->aux, nullptr);
+      if (!st && o.scoo_sort_cols && nnz) {
+        st = mfp_dev_scoo_sort_cols(vt, rows, cols, prm.slice_size, nnz, m->vals, m->cols_a, m->rows_a, nullptr);
+        m->rows_unsorted = true;
+      }
       if (!st) st = mfp_dev_scoo_x_windows(nnz, m->cols_a, m->aux, m->slices, dwin, nullptr);
       if (!st && (cudaMemcpy(win.data(), dwin, win.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
                   cudaMemcpy(hsp.data(), m->aux, hsp.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess))
@@ -1476,6 +1499,13 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                  : coo_spmv<float>(m->rows, (uint32_t)m->nnz, (const float *)m->vals, m->cols_a, m->rows_a,
                                    (const float *)x, (float *)y, m->ws, m->ws_bytes, stream);
     case MFP_FORMAT_SCOO:
+      if (m->rows_unsorted)
+        return f64 ? scoo_spmv<double, true>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
+                                             m->rows_a, m->aux, m->win, m->max_window, m->order, (const double *)x,
+                                             (double *)y, stream)
+                   : scoo_spmv<float, true>(m->rows, m->slices, m->slice_size, (const float *)m->vals, m->cols_a,
+                                            m->rows_a, m->aux, m->win, m->max_window, m->order, (const float *)x,
+                                            (float *)y, stream);
       return f64 ? scoo_spmv<double>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
                                      m->rows_a, m->aux, m->win, m->max_window, m->order, (const double *)x,
                                      (double *)y, stream)

@@ -704,6 +704,34 @@ int coo_from_csr_t(uint32_t rows, const uint32_t *rp, const uint32_t *ci, const 
   return ok();
 }
 
+// Stable LSD radix sort of n (key, payload) pairs on the low `bits` key bits;
+// k0 / p0 hold the input and, on return, the sorted pairs (buffers swap).
+template <typename P>
+int radix_sort_pairs(uint32_t n, uint32_t bits, unsigned long long *&k0, P *&p0, scratch &sc) {
+  if (n == 0 || bits == 0) return MFP_SUCCESS;
+  const uint32_t tiles = blocks_for(n, kRadixTile);
+  const uint64_t ncount = 256ull * tiles;
+  if (ncount > 0xffffffffull) return fail(MFP_ERROR_TOO_LARGE, "too many radix tiles");
+  unsigned long long *k1 = nullptr;
+  P *p1 = nullptr;
+  uint32_t *hist = nullptr, *hoff = nullptr;
+  int s;
+  if ((s = sc.get(&k1, n)) || (s = sc.get(&p1, n)) || (s = sc.get(&hist, ncount)) || (s = sc.get(&hoff, ncount + 1)))
+    return s;
+  const size_t smem = sizeof(radix_smem<P>);
+  CV_TRY(cudaFuncSetAttribute(radix_scatter_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+         "cudaFuncSetAttribute");
+  for (uint32_t shift = 0; shift < bits; shift += 8) {
+    radix_hist_kernel<<<tiles, kThreads, 0, sc.st>>>(n, k0, shift, tiles, hist);
+    if ((s = exclusive_scan((uint32_t)ncount, f_counts{hist}, hoff, sc))) return s;
+    radix_scatter_kernel<P><<<tiles, kThreads, smem, sc.st>>>(n, k0, p0, shift, tiles, hoff, k1, p1);
+    CV_TRY(cudaGetLastError(), "radix pass");
+    std::swap(k0, k1);
+    std::swap(p0, p1);
+  }
+  return MFP_SUCCESS;
+}
+
 template <typename T>
 int csr_from_coo_t(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *ri, const uint32_t *ci,
                    const double *v, uint32_t *rp, uint32_t *co, T *data, void *stream) {
@@ -718,8 +746,8 @@ int csr_from_coo_t(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *r
   }
   const uint32_t rb = rows > 1 ? bits_for(rows - 1) : 0u, cb = cols > 1 ? bits_for(cols - 1) : 0u;
   uint32_t *err = nullptr;
-  unsigned long long *k0 = nullptr, *k1 = nullptr;
-  T *p0 = nullptr, *p1 = nullptr;
+  unsigned long long *k0 = nullptr;
+  T *p0 = nullptr;
   int s;
   if ((s = sc.get(&err, 4)) || (s = sc.get(&k0, nnz)) || (s = sc.get(&p0, nnz))) return s;
   const uint32_t err_init[4] = {0u, 0xffffffffu, 0u, 0u};
@@ -732,29 +760,64 @@ int csr_from_coo_t(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *r
   CV_TRY(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   if (h_err[0] & 1u) return fail(MFP_ERROR_INVALID_VALUE, "row id >= rows %u at element %u", rows, h_err[1]);
   if (h_err[0] & 2u) return fail(MFP_ERROR_INVALID_VALUE, "col id >= cols %u at element %u", cols, h_err[1]);
-  if (h_err[2]) {  // not in CSR order: stable sort on (row, col); in order already, a stable sort keeps it
-    const uint32_t tiles = blocks_for(nnz, kRadixTile);
-    const uint64_t ncount = 256ull * tiles;
-    if (ncount > 0xffffffffull) return fail(MFP_ERROR_TOO_LARGE, "too many radix tiles");
-    uint32_t *hist = nullptr, *hoff = nullptr;
-    if ((s = sc.get(&k1, nnz)) || (s = sc.get(&p1, nnz)) || (s = sc.get(&hist, ncount)) ||
-        (s = sc.get(&hoff, ncount + 1)))
-      return s;
-    const size_t smem = sizeof(radix_smem<T>);
-    CV_TRY(cudaFuncSetAttribute(radix_scatter_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-           "cudaFuncSetAttribute");
-    for (uint32_t shift = 0; shift < rb + cb; shift += 8) {
-      radix_hist_kernel<<<tiles, kThreads, 0, st>>>(nnz, k0, shift, tiles, hist);
-      if ((s = exclusive_scan((uint32_t)ncount, f_counts{hist}, hoff, sc))) return s;
-      radix_scatter_kernel<T><<<tiles, kThreads, smem, st>>>(nnz, k0, p0, shift, tiles, hoff, k1, p1);
-      CV_TRY(cudaGetLastError(), "radix pass");
-      std::swap(k0, k1);
-      std::swap(p0, p1);
-    }
-  }
+  // not in CSR order: stable sort on (row, col); in order already, a stable sort would keep it
+  if (h_err[2] && (s = radix_sort_pairs<T>(nnz, rb + cb, k0, p0, sc))) return s;
   rowptr_from_keys_kernel<<<blocks_for((uint64_t)nnz + 1, kThreads), kThreads, 0, st>>>(nnz, rows, k0, cb, rp);
   csr_split_kernel<T><<<blocks_for(nnz, kThreads), kThreads, 0, st>>>(nnz, k0, p0, (1ull << cb) - 1ull, co, data);
   CV_TRY(cudaGetLastError(), "csr_split_kernel");
+  CV_TRY(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return ok();
+}
+
+// SCOO sort_cols: keys (slice << cb | col) with the element index as payload;
+// after the stable sort, values and rows are gathered by index.
+__global__ void __launch_bounds__(kThreads) slice_keys_kernel(uint32_t nnz, const uint32_t *__restrict__ ri,
+                                                              const uint32_t *__restrict__ ci, uint32_t slice_size,
+                                                              uint32_t cb, unsigned long long *__restrict__ keys,
+                                                              uint32_t *__restrict__ idx) {
+  const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= nnz) return;
+  keys[i] = ((unsigned long long)(ri[i] / slice_size) << cb) | ci[i];
+  idx[i] = i;
+}
+template <typename T>
+__global__ void __launch_bounds__(kThreads) slice_gather_kernel(uint32_t nnz, const unsigned long long *__restrict__ keys,
+                                                                const uint32_t *__restrict__ idx,
+                                                                unsigned long long cmask, const T *__restrict__ v_in,
+                                                                const uint32_t *__restrict__ r_in, T *__restrict__ v_out,
+                                                                uint32_t *__restrict__ c_out, uint32_t *__restrict__ r_out) {
+  const uint32_t p = blockIdx.x * kThreads + threadIdx.x;
+  if (p >= nnz) return;
+  const uint32_t j = idx[p];
+  c_out[p] = (uint32_t)(keys[p] & cmask);
+  v_out[p] = v_in[j];
+  r_out[p] = r_in[j];
+}
+
+template <typename T>
+int scoo_sort_cols_t(uint32_t rows, uint32_t cols, uint32_t slice_size, uint32_t nnz, T *v, uint32_t *ci,
+                     uint32_t *ri, cudaStream_t st) {
+  scratch sc(st);
+  if (nnz == 0) return ok();
+  if (!v || !ci || !ri) return fail(MFP_ERROR_INVALID_VALUE, "null array");
+  if (slice_size == 0) return fail(MFP_ERROR_INVALID_VALUE, "slice_size 0");
+  const uint32_t cb = cols > 1 ? bits_for(cols - 1) : 0u;
+  const uint32_t sb = rows > slice_size ? bits_for((rows - 1) / slice_size) : 0u;
+  unsigned long long *k0 = nullptr;
+  uint32_t *p0 = nullptr;
+  T *vcopy = nullptr;
+  uint32_t *rcopy = nullptr;
+  int s;
+  if ((s = sc.get(&k0, nnz)) || (s = sc.get(&p0, nnz)) || (s = sc.get(&vcopy, nnz)) || (s = sc.get(&rcopy, nnz)))
+    return s;
+  CV_TRY(cudaMemcpyAsync(vcopy, v, (size_t)nnz * sizeof(T), cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+  CV_TRY(cudaMemcpyAsync(rcopy, ri, (size_t)nnz * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+  slice_keys_kernel<<<blocks_for(nnz, kThreads), kThreads, 0, st>>>(nnz, ri, ci, slice_size, cb, k0, p0);
+  CV_TRY(cudaGetLastError(), "slice_keys_kernel");
+  if ((s = radix_sort_pairs<uint32_t>(nnz, sb + cb, k0, p0, sc))) return s;
+  slice_gather_kernel<T><<<blocks_for(nnz, kThreads), kThreads, 0, st>>>(nnz, k0, p0, (1ull << cb) - 1ull, vcopy, rcopy,
+                                                                         v, ci, ri);
+  CV_TRY(cudaGetLastError(), "slice_gather_kernel");
   CV_TRY(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   return ok();
 }
@@ -897,6 +960,16 @@ int mfp_dev_scoo_from_csr(int vt, uint32_t rows, uint32_t nnz, const uint32_t *r
   CV_TRY(cudaGetLastError(), "scoo_slices_kernel");
   // values, c_index and r_index are the CSR arrays in CSR order with row ids
   return mfp_dev_coo_from_csr(vt, rows, rp, ci, vals, 0, ov, oc, orow, stream);
+}
+
+int mfp_dev_scoo_sort_cols(int vt, uint32_t rows, uint32_t cols, uint32_t slice_size, uint32_t nnz, void *values,
+                           uint32_t *c_index, uint32_t *r_index, void *stream) {
+  if (!valid_vt(vt)) return fail(MFP_ERROR_INVALID_VALUE, "bad value type");
+  if (vt == MFP_F64)
+    return scoo_sort_cols_t<double>(rows, cols, slice_size, nnz, static_cast<double *>(values), c_index, r_index,
+                                    as_stream(stream));
+  return scoo_sort_cols_t<float>(rows, cols, slice_size, nnz, static_cast<float *>(values), c_index, r_index,
+                                 as_stream(stream));
 }
 
 int mfp_dev_scoo_x_windows(uint32_t nnz, const uint32_t *ci, const uint32_t *sp, uint32_t slices, uint32_t *win,

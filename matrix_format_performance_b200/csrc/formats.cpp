@@ -146,6 +146,35 @@ int scoo_from_csr(uint32_t rows, const uint32_t *rp, const uint32_t *columns, co
   return ok();
 }
 
+// The reference's disabled sort_cols block (scoo_matrix_class.cpp:102-138):
+// each slice's elements ordered by column.  The reference sorts a permutation
+// with std::sort, which is not stable, so its order between equal columns is
+// unspecified; this restatement sorts stably (equal columns keep CSR order).
+template <typename T>
+int scoo_sort_cols(uint32_t slices, const uint32_t *sp, T *values, uint32_t *ci, uint32_t *ri) {
+  if (!sp) return fail(MFP_ERROR_INVALID_VALUE, "null slices_ptr");
+  std::vector<uint32_t> perm, tc, tr;
+  std::vector<T> tv;
+  for (uint32_t s = 0; s < slices; ++s) {
+    const uint32_t b = sp[s], e = sp[s + 1];
+    if (b >= e) continue;
+    if (!values || !ci || !ri) return fail(MFP_ERROR_INVALID_VALUE, "null array");
+    const uint32_t n = e - b;
+    perm.resize(n);
+    std::iota(perm.begin(), perm.end(), 0u);
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t l, uint32_t r) { return ci[b + l] < ci[b + r]; });
+    tv.assign(values + b, values + e);
+    tc.assign(ci + b, ci + e);
+    tr.assign(ri + b, ri + e);
+    for (uint32_t k = 0; k < n; ++k) {
+      values[b + k] = tv[perm[k]];
+      ci[b + k] = tc[perm[k]];
+      ri[b + k] = tr[perm[k]];
+    }
+  }
+  return ok();
+}
+
 template <typename T>
 int compare(uint32_t n, const T *a, const T *b, double *error, uint32_t *first_bad) {
   if (!a || !b || !error) return fail(MFP_ERROR_INVALID_VALUE, "null array");
@@ -297,6 +326,13 @@ int mfp_scoo_from_csr_f32(uint32_t rows, const uint32_t *rp, const uint32_t *c, 
 int mfp_scoo_from_csr_f64(uint32_t rows, const uint32_t *rp, const uint32_t *c, const double *d,
                           const mfp_scoo_params *p, double *v, uint32_t *ci, uint32_t *ri, uint32_t *sp) {
   return scoo_from_csr<double>(rows, rp, c, d, p, v, ci, ri, sp);
+}
+
+int mfp_scoo_sort_cols_f32(uint32_t slices, const uint32_t *sp, float *v, uint32_t *ci, uint32_t *ri) {
+  return scoo_sort_cols<float>(slices, sp, v, ci, ri);
+}
+int mfp_scoo_sort_cols_f64(uint32_t slices, const uint32_t *sp, double *v, uint32_t *ci, uint32_t *ri) {
+  return scoo_sort_cols<double>(slices, sp, v, ci, ri);
 }
 
 // fill_row_blocks — csr_adaptive_spmv.cu:180-240: close a bin when its

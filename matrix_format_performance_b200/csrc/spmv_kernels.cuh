@@ -1302,6 +1302,70 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4
 }
 
 
+// SCOO with the slices' elements in column order (the reference's sort_cols
+// layout, scoo_matrix_class.cpp:102-138): rows are not contiguous within a
+// slice, so each product is added into its row's shared-memory accumulator
+// with an atomic, as the reference's scoo_spmv_kernel does (gpu/scoo_spmv.cu:
+// 46-129).  Column order makes the x reads of a slice ascend.  The order of the
+// additions into a row is not fixed.
+template <typename T, bool XWIN>
+__global__ void __launch_bounds__(kBlock) scoo_unsorted_kernel(uint32_t n_rows, uint32_t slice_size,
+                                                               const T *__restrict__ vals,
+                                                               const uint32_t *__restrict__ cidx,
+                                                               const uint32_t *__restrict__ ridx,
+                                                               const uint32_t *__restrict__ slices_ptr,
+                                                               const uint32_t *__restrict__ windows,
+                                                               uint32_t max_window,
+                                                               const uint32_t *__restrict__ order,
+                                                               const T *__restrict__ x, T *__restrict__ y) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  T *acc = reinterpret_cast<T *>(dyn);
+  T *s_x = acc + ((slice_size + 3u) & ~3u);
+  const uint64_t pol = policy_evict_first();
+  const uint32_t s = order ? order[blockIdx.x] : blockIdx.x;
+  const uint32_t row0 = s * slice_size;
+  if (row0 >= n_rows) return;
+  const uint32_t nrows = min(slice_size, n_rows - row0);
+  const uint32_t eb = slices_ptr[s], ee = slices_ptr[s + 1];
+  for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) acc[i] = T(0);
+  bool use_win = false;
+  uint32_t wlo = 0;
+  if (XWIN && eb < ee) {
+    wlo = windows[2 * s];
+    const uint32_t whi = windows[2 * s + 1];
+    if (whi > wlo && whi - wlo <= max_window) {
+      use_win = true;
+      for (uint32_t i = threadIdx.x; i < whi - wlo; i += kBlock) s_x[i] = ld_x(x + wlo + i);
+    }
+  }
+  __syncthreads();
+  // 4 elements per thread in flight, coalesced across the CTA
+  for (uint32_t e0 = eb + threadIdx.x; e0 < ee; e0 += 4u * kBlock) {
+    T v[4];
+    uint32_t c[4], r[4];
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t e = e0 + k * kBlock;
+      if (e < ee) {
+        v[k] = ld_stream1(vals + e, pol);
+        c[k] = ld_stream1(cidx + e, pol);
+        r[k] = ld_stream1(ridx + e, pol);
+      }
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t e = e0 + k * kBlock;
+      if (e < ee) {
+        const T xv = (XWIN && use_win) ? s_x[c[k] - wlo] : ld_x(x + c[k]);
+        const uint32_t lr = r[k] - row0;
+        if (lr < nrows) atomicAdd(&acc[lr], mul_rn(v[k], xv));
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
+}
+
 template <typename T>
 __global__ void fill_kernel(uint64_t n, T *v, T value) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)

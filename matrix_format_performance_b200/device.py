@@ -143,12 +143,15 @@ class DeviceMatrix:
 
     @classmethod
     def from_device_csr(cls, row_ptr, columns, data, cols: int, fmt: int, *, config: dict | None = None,
-                        ell_width: int | None = None, scoo: "_capi.ScooParams | None" = None) -> "DeviceMatrix":
+                        ell_width: int | None = None, scoo: "_capi.ScooParams | None" = None,
+                        scoo_sort_cols: bool = False) -> "DeviceMatrix":
         """Builds format `fmt` from a CSR already on the GPU (torch tensors):
         the layout is converted by the engine's kernels (mfp_matrix_create_device).
-        ell_width: ELL / hybrid ELL part (None = longest row)."""
+        ell_width: ELL / hybrid ELL part (None = longest row); scoo_sort_cols: the
+        SCOO slices in column order."""
         o = _capi.DeviceBuildOptions()
         o.ell_width = _capi.ELL_WIDTH_LONGEST if ell_width is None else int(ell_width)
+        o.scoo_sort_cols = int(bool(scoo_sort_cols))
         cfg = _capi.CsrConfig()
         if config:
             for k, v in config.items():

@@ -168,9 +168,10 @@ def row_length_quantile(m: csr_matrix_class, q: float) -> int:
 
 
 class scoo_matrix_class:
-    """scoo_matrix_class<T> (scoo_matrix_class.cpp:58-139)."""
+    """scoo_matrix_class<T> (scoo_matrix_class.cpp:58-139).  sort_cols=True applies
+    the reference's disabled sort_cols block (:102-138) with a stable sort."""
 
-    def __init__(self, sm_count: int, shared_mem_size: int, m: csr_matrix_class):
+    def __init__(self, sm_count: int, shared_mem_size: int, m: csr_matrix_class, sort_cols: bool = False):
         self.rows, self.cols, self.dtype, self.nnz = m.rows, m.cols, m.dtype, m.nnz
         p = _capi.ScooParams()
         call("mfp_scoo_params_compute", m.rows, sm_count, shared_mem_size, _VT[self.dtype], C.byref(p))
@@ -182,6 +183,10 @@ class scoo_matrix_class:
         self.slices_ptr = np.empty(p.slices_count + 1, np.uint32)
         call(f"mfp_scoo_from_csr_{_SFX[self.dtype]}", m.rows, ptr(m.row_ptr), ptr(m.columns), ptr(m.data),
              C.byref(p), ptr(self.values), ptr(self.c_index), ptr(self.r_index), ptr(self.slices_ptr))
+        self.sort_cols = bool(sort_cols)
+        if sort_cols:
+            call(f"mfp_scoo_sort_cols_{_SFX[self.dtype]}", p.slices_count, ptr(self.slices_ptr), ptr(self.values),
+                 ptr(self.c_index), ptr(self.r_index))
 
 
 def fill_row_blocks(m: csr_matrix_class, nnz_per_wg: int = 64) -> np.ndarray:

@@ -256,15 +256,16 @@ measurement_class gpu_scoo_spmv(bool print_diff, const scoo_matrix_class<data_ty
   return mfp_host::timed_spmv<data_type>(
       "GPU SCOO", meta, x, y, reusable_vector, reference_y, print_diff, mfp_host::model_bytes<data_type>(meta),
       2.0 * nnz, [&] {
+        // the sort_cols layout has rows in any order within a slice
+        auto f32 = matrix.cols_sorted ? mfp_scoo_spmv_unsorted_f32 : mfp_scoo_spmv_f32;
+        auto f64 = matrix.cols_sorted ? mfp_scoo_spmv_unsorted_f64 : mfp_scoo_spmv_f64;
         return sizeof(data_type) == 4
-                   ? mfp_scoo_spmv_f32(meta.rows_count, meta.cols_count, slices, matrix.slice_size,
-                                       (const float *)A.get(), c_index.get(), r_index.get(), sp.as<uint32_t>(),
-                                       dwin.as<uint32_t>(), max_window, dord.as<uint32_t>(),
-                                       (const float *)x.get(), (float *)y.get(), nullptr)
-                   : mfp_scoo_spmv_f64(meta.rows_count, meta.cols_count, slices, matrix.slice_size,
-                                       (const double *)A.get(), c_index.get(), r_index.get(), sp.as<uint32_t>(),
-                                       dwin.as<uint32_t>(), max_window, dord.as<uint32_t>(),
-                                       (const double *)x.get(), (double *)y.get(), nullptr);
+                   ? f32(meta.rows_count, meta.cols_count, slices, matrix.slice_size, (const float *)A.get(),
+                         c_index.get(), r_index.get(), sp.as<uint32_t>(), dwin.as<uint32_t>(), max_window,
+                         dord.as<uint32_t>(), (const float *)x.get(), (float *)y.get(), nullptr)
+                   : f64(meta.rows_count, meta.cols_count, slices, matrix.slice_size, (const double *)A.get(),
+                         c_index.get(), r_index.get(), sp.as<uint32_t>(), dwin.as<uint32_t>(), max_window,
+                         dord.as<uint32_t>(), (const double *)x.get(), (double *)y.get(), nullptr);
       });
 }
 

@@ -13,8 +13,11 @@ template <typename data_type>
 class scoo_matrix_class {
  public:
   scoo_matrix_class() = delete;
-  explicit scoo_matrix_class(unsigned int sm_count, size_t shared_mem_size, csr_matrix_class<data_type> &matrix)
-      : meta(matrix.meta) {
+  // sort_cols: the reference's disabled option (scoo_matrix_class.cpp:102-138),
+  // each slice in column order (stable sort; the reference's is not stable)
+  explicit scoo_matrix_class(unsigned int sm_count, size_t shared_mem_size, csr_matrix_class<data_type> &matrix,
+                             bool sort_cols = false)
+      : meta(matrix.meta), cols_sorted(sort_cols) {
     mfp_scoo_params p{};
     mfp_host::check(mfp_scoo_params_compute(meta.rows_count, sm_count, shared_mem_size,
                                             mfp_host::vt<data_type>::value, &p),
@@ -36,9 +39,17 @@ class scoo_matrix_class {
                                          (const double *)matrix.data.get(), &p, (double *)values.get(),
                                          c_index.get(), r_index.get(), slices_ptr.get());
     mfp_host::check(st, "scoo_matrix_class");
+    if (sort_cols) {
+      st = sizeof(data_type) == 4 ? mfp_scoo_sort_cols_f32(slices_count, slices_ptr.get(), (float *)values.get(),
+                                                           c_index.get(), r_index.get())
+                                  : mfp_scoo_sort_cols_f64(slices_count, slices_ptr.get(), (double *)values.get(),
+                                                           c_index.get(), r_index.get());
+      mfp_host::check(st, "scoo_matrix_class sort_cols");
+    }
   }
 
   const matrix_market::matrix_class::matrix_meta meta;
+  const bool cols_sorted;  // engine extension: true for the sort_cols layout
 
  public:
   unsigned int slices_count{};

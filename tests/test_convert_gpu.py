@@ -336,3 +336,17 @@ def test_scratch_pool_is_kept_and_released():
     assert convert.scratch_bytes() >= m.nnz * 16  # keys and payloads of both sort buffers stay mapped
     convert.release_scratch()
     assert convert.scratch_bytes() == 0
+
+
+@pytest.mark.parametrize("name", ["laplacian_512", "power_law_300k", "stencil_40", "sparse_rows", "one_row",
+                                  "empty_matrix"])
+@pytest.mark.parametrize("dt", DTS)
+def test_scoo_sort_cols_on_device_identical(name, dt):
+    m = mat(name, dt)
+    want = F.scoo_matrix_class(148, 49152, m, sort_cols=True)
+    plain = F.scoo_matrix_class(148, 49152, m)
+    v, c, r = dev(plain.values), dev(plain.c_index), dev(plain.r_index)
+    convert.scoo_sort_cols(v, c, r, m.rows, m.cols, plain.slice_size)
+    np.testing.assert_array_equal(host(c), want.c_index)
+    np.testing.assert_array_equal(host(r), want.r_index)
+    np.testing.assert_array_equal(bits(host(v)), bits(want.values))

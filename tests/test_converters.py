@@ -7,6 +7,7 @@ import pytest
 
 from conftest import golden_cases, load_golden
 from matrix_format_performance_b200 import formats as F
+from matrix_format_performance_b200 import synth
 from matrix_format_performance_b200._capi import MfpError
 
 
@@ -118,3 +119,28 @@ def test_compare_results_matches_reference_rule():
     b[1] = 2.5
     err, bad = F.compare_results(b, a)
     assert err == pytest.approx(0.25 / 14.0) and bad == 1
+
+
+@pytest.mark.parametrize("kind", ["power_law", "stencil", "banded"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_scoo_sort_cols_orders_each_slice_by_column_stably(kind, dt):
+    """The reference's disabled sort_cols block (scoo_matrix_class.cpp:102-138)
+    restated with a stable sort: per slice, the elements ordered by column,
+    equal columns in CSR order; slices_ptr and parameters unchanged."""
+    m = {"power_law": lambda: synth.power_law(rows=40_000, seed=3),
+         "stencil": lambda: synth.stencil_27(24, seed=1),
+         "banded": lambda: synth.banded(n=30_000, seed=2)}[kind]().astype(dt)
+    plain = F.scoo_matrix_class(148, 49152, m)
+    srt = F.scoo_matrix_class(148, 49152, m, sort_cols=True)
+    np.testing.assert_array_equal(srt.slices_ptr, plain.slices_ptr)
+    assert (srt.slices_count, srt.slice_size, srt.lane_size) == (plain.slices_count, plain.slice_size,
+                                                                   plain.lane_size)
+    sp = plain.slices_ptr
+    for s in range(plain.slices_count):
+        b, e = int(sp[s]), int(sp[s + 1])
+        if b >= e:
+            continue
+        p = np.argsort(plain.c_index[b:e], kind="stable")
+        np.testing.assert_array_equal(srt.c_index[b:e], plain.c_index[b:e][p])
+        np.testing.assert_array_equal(srt.r_index[b:e], plain.r_index[b:e][p])
+        np.testing.assert_array_equal(srt.values[b:e].view(np.uint8), plain.values[b:e][p].view(np.uint8))
