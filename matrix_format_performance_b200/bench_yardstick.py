@@ -1,9 +1,10 @@
 """The engine's formats beside cuSPARSE's generic SpMV (the vendor yardstick).
 
     python -m matrix_format_performance_b200.bench_yardstick [--rows 4194304] [--stencil 128] [--banded 8388608]
-        [--which power_law,stencil,banded]
+        [--which power_law,stencil,banded] [--dtype f32|f64]
 
-For the power-law, stencil and banded matrices (FP32): median device time of
+For the power-law, stencil and banded matrices (FP32, or FP64 with --dtype
+f64): median device time of
 the engine's CSR scalar / vector / adaptive, COO, SCOO (also with each slice in
 column order, the reference's disabled sort_cols option) and hybrid kernels and
 of cusparseSpMV on CSR (default, ALG1, ALG2) and COO (default), 20 launches
@@ -26,10 +27,12 @@ def measure(name, m, reps=20):
     from . import yardstick as Y
     from .device import FORMAT_NAMES, LABELS, DeviceMatrix, device_info
     dev = device_info(0)
-    nbytes = m.nnz * 8 + (m.rows + 1) * 4 + m.cols * 4 + m.rows * 4
-    x = torch.from_numpy(synth.vector(5, m.cols).astype(np.float32)).cuda()
-    y = torch.empty(m.rows, device="cuda")
-    out = {"matrix": name, "rows": m.rows, "nnz": int(m.nnz), "engine": {}, "cusparse": {}}
+    vs = m.data.dtype.itemsize
+    nbytes = m.nnz * (vs + 4) + (m.rows + 1) * 4 + m.cols * vs + m.rows * vs
+    x = torch.from_numpy(synth.vector(5, m.cols).astype(m.data.dtype)).cuda()
+    y = torch.empty(m.rows, dtype=x.dtype, device="cuda")
+    out = {"matrix": name, "dtype": str(m.data.dtype), "rows": m.rows, "nnz": int(m.nnz), "engine": {},
+           "cusparse": {}}
     for key in ("csr", "csr_vector", "csr_adaptive", "coo", "scoo", "hybrid"):
         fmt = FORMAT_NAMES[key]
         dm = DeviceMatrix.build(m, fmt, sm_count=dev.sm_count, shared_mem=int(dev.shared_mem_per_block),
@@ -62,6 +65,7 @@ def main() -> None:
     ap.add_argument("--stencil", type=int, default=128)
     ap.add_argument("--banded", type=int, default=8_388_608)
     ap.add_argument("--which", default="power_law,stencil,banded")
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
     a = ap.parse_args()
     import torch
 
@@ -72,7 +76,8 @@ def main() -> None:
                            ("stencil", f"stencil27_{a.stencil}", lambda: synth.stencil_27(a.stencil)),
                            ("banded", f"banded_{a.banded}", lambda: synth.banded(n=a.banded))):
         if key in which:
-            print(json.dumps(measure(name, gen().astype(np.float32))), flush=True)
+            print(json.dumps(measure(name, gen().astype(np.float64 if a.dtype == "f64" else np.float32))),
+                  flush=True)
 
 
 if __name__ == "__main__":

@@ -39,10 +39,26 @@ namespace dev {
 #ifndef MFP_CSR_MINBLOCKS
 #define MFP_CSR_MINBLOCKS 8
 #endif
+// CTAs per SM the FP32 CSR vector kernel and the FP64 CSR kernels (scalar;
+// vector and adaptive) are register-limited to.  Measured on the power-law,
+// stencil and banded matrices in FP64: 5 for scalar (48 registers instead of
+// 40 with spills) and 6 for the others are fastest.
+#ifndef MFP_CSR_MINBLOCKS_VEC
+#define MFP_CSR_MINBLOCKS_VEC 6
+#endif
+#ifndef MFP_CSR_MINBLOCKS64
+#define MFP_CSR_MINBLOCKS64 5
+#endif
+#ifndef MFP_CSR_MINBLOCKS64_OTHER
+#define MFP_CSR_MINBLOCKS64_OTHER 6
+#endif
 // CTAs per SM the register-resident COO / SCOO kernels are register-limited
-// to (FP32; FP64 uses 4).
+// to, FP32 and FP64 (FP64: 5 measured faster than 4 and 6).
 #ifndef MFP_COO_MINBLOCKS
 #define MFP_COO_MINBLOCKS 6
+#endif
+#ifndef MFP_COO_MINBLOCKS64
+#define MFP_COO_MINBLOCKS64 5
 #endif
 #ifndef MFP_PIECES_FIRST
 #define MFP_PIECES_FIRST 0
@@ -844,7 +860,7 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
 }
 
 template <typename T, int ALGO, bool VEC>
-__global__ void __launch_bounds__(kBlock, (sizeof(T) == 4 && ALGO != 1) ? MFP_CSR_MINBLOCKS : 6) csr_kernel(const csr_args<T> A) {
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? (ALGO != 1 ? MFP_CSR_MINBLOCKS : MFP_CSR_MINBLOCKS_VEC) : (ALGO == 0 ? MFP_CSR_MINBLOCKS64 : MFP_CSR_MINBLOCKS64_OTHER)) csr_kernel(const csr_args<T> A) {
   __shared__ csr_smem<T> sm;
   const uint64_t pol = policy_evict_first();
   // the hardware starts blocks in index order: with A.order the heaviest work
@@ -942,7 +958,7 @@ struct coo_smem {
 // without elements untouched (the COO tail of the hybrid format, after the
 // ELL kernel has written every row).
 template <typename T, bool VEC, bool ACCUM = false>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4) coo_kernel(uint32_t n_rows, uint32_t nnz,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64) coo_kernel(uint32_t n_rows, uint32_t nnz,
                                                      const T *__restrict__ vals,
                                                      const uint32_t *__restrict__ cols,
                                                      const uint32_t *__restrict__ rows,
@@ -1090,7 +1106,6 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
   T sf = T(0), sl = T(0);
   if (active) {
     rf = rw[0];
-    rl = rw[cnt - 1u];
     uint32_t cur = rf;
     T acc = pr[0];
     bool first = true;
@@ -1112,6 +1127,7 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
     }
     if (first) sf = acc;
     sl = acc;
+    rl = cur;  // the last run's row (no dynamic index: rw stays in registers)
   }
   const bool single = active && rf == rl;
   const uint32_t prev_last = __shfl_up_sync(0xffffffffu, rl, 1);
@@ -1174,7 +1190,7 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
 }
 
 template <typename T, bool VEC, bool ACCUM>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4)
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
                     coo_carry<T> cw) {
@@ -1245,7 +1261,7 @@ struct scoo_smem_static {
 };
 
 template <typename T, bool VEC, bool XWIN>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : 4) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,
                                                       const uint32_t *__restrict__ ridx,
