@@ -57,3 +57,26 @@ def test_invalid_arguments_are_reported_without_gpu():
     n = C.c_size_t()
     call("mfp_coo_workspace_bytes", 10, 5000, C.byref(n))
     assert n.value == 16 + 20 * 24  # a header, then 24 bytes per 256-element warp tile
+
+
+def test_device_converters_check_arguments_without_gpu():
+    """The on-device converters reject bad arguments before any CUDA call."""
+    with pytest.raises(MfpError, match="bad value type"):
+        call("mfp_dev_ell_from_csr", 7, 1, None, None, None, 1, None, None, None)
+    with pytest.raises(MfpError, match="bad value type"):
+        call("mfp_dev_csr_from_coo", 9, 1, 1, 0, None, None, None, None, None, None, None)
+    with pytest.raises(MfpError, match="bad value type"):
+        call("mfp_dev_scoo_sort_cols", 4, 1, 1, 1, 0, None, None, None, None)
+    with pytest.raises(MfpError, match="null"):
+        call("mfp_dev_rows_statistics", 4, None, None, None)
+    with pytest.raises(MfpError, match="bad format or value type"):
+        call("mfp_matrix_create_device", 11, 0, 1, 1, 0, None, None, None, None, C.byref(C.c_void_p()))
+    rp = np.array([0, 1], np.uint32)
+    with pytest.raises(MfpError, match="slice_size 0"):
+        call("mfp_dev_scoo_from_csr", 0, 1, 1, C.c_void_p(rp.ctypes.data), None, None,
+             C.byref(_capi.ScooParams(4, 0, 1)), None, None, None, C.c_void_p(rp.ctypes.data), None)
+
+
+def test_host_scoo_sort_cols_checks_arguments():
+    with pytest.raises(MfpError, match="null slices_ptr"):
+        call("mfp_scoo_sort_cols_f32", 1, None, None, None, None)
