@@ -336,11 +336,11 @@ int mfp_scoo_spmv_unsorted_f64(uint32_t rows, uint32_t cols, uint32_t slices_cou
                                const uint32_t *slice_order, const double *x, double *y, void *stream);
 
 /* Hybrid ELL + COO — counterpart of gpu_hybrid_spmv / gpu_hybrid_atomic_spmv
- * (gpu_matrix_multiplier.cu:866-1096).  Two launches: the ELL kernel writes
- * every row's ELL part, then the tile-based COO kernel adds the tail (the
- * elements past the ELL width, hybrid_matrix_class's coo_matrix) row by row,
- * without atomics.  `workspace` is the COO look-back workspace of the tail
- * (mfp_hybrid_workspace_bytes; zero-filled before first use, left zeroed). */
+ * (gpu_matrix_multiplier.cu:866-1096).  The ELL kernel writes every row's ELL
+ * part, then the two-pass COO adds the tail (the elements past the ELL width,
+ * hybrid_matrix_class's coo_matrix) row by row, without atomics: three
+ * launches.  `workspace` holds the tail's warp-tile partial sums
+ * (mfp_hybrid_workspace_bytes; no initialisation needed). */
 int mfp_hybrid_workspace_bytes(uint32_t rows, uint32_t coo_nnz, size_t *bytes);
 int mfp_hybrid_spmv_f32(uint32_t rows, uint32_t cols, uint32_t ell_width, const float *ell_data,
                         const uint32_t *ell_cols, uint32_t coo_nnz, const float *coo_data,

@@ -14,16 +14,20 @@
 //                 (gpu/csr_adaptive_spmv.cu:26-178)
 //   ELL           one thread per row over column-major slots
 //                 (gpu/gpu_matrix_multiplier.cu:450-471)
-//   COO           tiles of consecutive elements, block segmented reduction,
-//                 rows shared by tiles combined by look-back
-//                 (replaces the atomics of gpu_matrix_multiplier.cu:622-638)
+//   COO           two passes: warp tiles of 256 consecutive elements reduce
+//                 their runs (shuffle segmented scan) and write inner rows;
+//                 a fix-up pass adds the rows that cross tiles (replaces the
+//                 atomics of gpu_matrix_multiplier.cu:622-638).  The
+//                 allocation-free entry point keeps a single-pass kernel
+//                 whose tiles combine shared rows by look-back.
 //   SCOO          one CTA per slice, shared-memory row accumulators and an
 //                 optional shared-memory copy of the slice's x window
-//                 (gpu/scoo_spmv.cu:46-129)
-//   HYB           the ELL kernel for the ELL part, then the COO kernel in
-//                 accumulate mode for the tail (two launches, as the
-//                 reference's gpu/gpu_matrix_multiplier.cu:969-1002, with
-//                 the tail's atomics replaced by the COO tile reduction)
+//                 (gpu/scoo_spmv.cu:46-129); the sort_cols layout adds into
+//                 the accumulators with shared-memory atomics
+//   HYB           the ELL kernel for the ELL part, then the two COO passes in
+//                 accumulate mode for the tail (the reference's
+//                 gpu/gpu_matrix_multiplier.cu:969-1002, with the tail's
+//                 atomics replaced by the COO reduction)
 // Rows longer than a plan threshold (CSR family) are cut into pieces that
 // run as extra CTAs of the same launch and meet in a partial-sum buffer.
 #pragma once

@@ -9,8 +9,8 @@
 //     (compare_results: an error above 1e-9 is reported on stderr);
 //   * the result is a measurement_class with the reference's label.
 // Temporaries the reference allocates per call (CSR-Adaptive row blocks, SCOO
-// slices_ptr) are per call here too: the CSR plan, the COO look-back
-// workspace, the SCOO slice pointers and x windows.  A failing CUDA or engine
+// slices_ptr) are per call here too: the CSR plan, the COO workspace (the
+// warp tiles' partial sums), the SCOO slice pointers and x windows.  A failing CUDA or engine
 // call throws std::runtime_error (the reference ignored CUDA status codes).
 // Bytes in measurement_class: the reference's per-format counts where it has
 // them (CSR, CSR vector, ELL, COO); where it reports 0 (CSR-Adaptive, SCOO,

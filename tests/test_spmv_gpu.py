@@ -158,7 +158,7 @@ def test_long_rows_split_and_repeatable(oracle_lib, dt, fmt):
     x = synth.vector(3, m.cols).astype(dt)
     ys = run(m, fmt, x, reps=3, hybrid_width=4)
     check_tol(oracle_lib, m, x, ys[0], f"long rows fmt{fmt}")
-    # deterministic: counters and look-back state reset between launches
+    # deterministic: plan counters reset between launches, sums in a fixed order
     assert np.array_equal(ys[0], ys[1]) and np.array_equal(ys[1], ys[2])
 
 
