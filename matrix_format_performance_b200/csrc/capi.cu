@@ -568,6 +568,31 @@ int fill(uint64_t n, T *v, T value, void *stream) {
   return check_launch("fill_kernel launch");
 }
 
+// Launches that follow another launch of the same call may start early
+// (programmatic dependent launch): their CTAs are placed while the preceding
+// kernel drains and wait for it in griddep_wait() before touching its output.
+#ifndef MFP_PDL
+#define MFP_PDL 1
+#endif
+template <typename... KArgs, typename... Args>
+cudaError_t launch_after(void (*k)(KArgs...), uint32_t grid, cudaStream_t s, Args &&...args) {
+  if (!MFP_PDL) {
+    k<<<grid, d::kBlock, 0, s>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(d::kBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 // COO workspace: a 16-byte header (its error word stays 0: the two-pass COO
 // has no waits) and, per 256-element warp tile, the head and tail partial
 // sums (8 bytes each, FP64-sized), the flags and the tail row.
@@ -602,17 +627,24 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
   const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
   cudaStream_t s = as_stream(stream);
-  if (vec)
-    d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
-  else
-    d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
-  int st = check_launch("coo_warp_kernel launch");
-  if (st) return st;
-  if (n_wt > 1) {
-    d::coo_fixup_kernel<T, ACCUM><<<ceil_div(n_wt, d::kBlock), d::kBlock, 0, s>>>(n_wt, cw, y);
-    st = check_launch("coo_fixup_kernel launch");
+  // the accumulating warp pass (hybrid tail) follows the ELL launch of the same call
+  cudaError_t e;
+  if (ACCUM)
+    e = vec ? launch_after(d::coo_warp_kernel<T, true, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw)
+            : launch_after(d::coo_warp_kernel<T, false, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw);
+  else {
+    if (vec)
+      d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+    else
+      d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+    e = cudaGetLastError();
   }
-  return st;
+  if (e != cudaSuccess) return cuda_fail(e, "coo_warp_kernel launch");
+  if (n_wt > 1) {
+    e = launch_after(d::coo_fixup_kernel<T, ACCUM>, ceil_div(n_wt, d::kBlock), s, n_wt, cw, y);
+    if (e != cudaSuccess) return cuda_fail(e, "coo_fixup_kernel launch");
+  }
+  return ok();
 }
 
 // Single pass: 2048-element tiles taken by ticket; a tile that ends a row

@@ -197,6 +197,11 @@ __device__ __forceinline__ bool wait_flag(const uint32_t *flag, uint32_t limit) 
   return false;
 }
 
+// Programmatic dependent launch: waits until the preceding kernel of the
+// stream has completed and its writes are visible (a no-op when the launch did
+// not allow early start).  Hardware-managed; not a poll on memory.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void store_release(uint32_t *flag, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
 }

@@ -1198,6 +1198,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
                     coo_carry<T> cw) {
+  if (ACCUM) griddep_wait();  // y holds the ELL part written by the preceding launch
   const uint64_t pol = policy_evict_first();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t wt = blockIdx.x * (kBlock / 32u) + (threadIdx.x >> 5);
@@ -1222,6 +1223,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
 template <typename T, bool ACCUM>
 __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, coo_carry<T> cw, T *__restrict__ y) {
   constexpr uint32_t B = MFP_FIXUP_BATCH;
+  griddep_wait();  // the warp pass's partial sums and rows of y
   const uint32_t w = blockIdx.x * kBlock + threadIdx.x;
   if (w >= n_tiles) return;
   const uint32_t f = cw.flags[w];
