@@ -270,7 +270,9 @@ int mfp_ell_spmv_f64(uint32_t rows, uint32_t cols, uint32_t width, const double 
  * elements and writes the rows inside them; a fix-up pass adds up the rows
  * that cross those tiles, from partial sums kept in `workspace` (device memory
  * of mfp_coo_workspace_bytes bytes; no initialisation needed).  Results are
- * deterministic.  Calls that share a workspace must not overlap on the GPU. */
+ * deterministic.  Calls that share a workspace must not overlap on the GPU.
+ * Row ids must be below `rows`; elements with a larger row id are dropped
+ * (never written).  Empty rows get 0. */
 int mfp_coo_workspace_bytes(uint32_t rows, uint32_t nnz, size_t *bytes);
 int mfp_coo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
                      const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
@@ -278,25 +280,37 @@ int mfp_coo_spmv_f32(uint32_t rows, uint32_t cols, uint32_t nnz, const float *da
 int mfp_coo_spmv_f64(uint32_t rows, uint32_t cols, uint32_t nnz, const double *data,
                      const uint32_t *col_ids, const uint32_t *row_ids, const double *x, double *y,
                      void *workspace, size_t workspace_bytes, void *stream);
-/* Reads a COO workspace's error word (non-zero: a bounded wait gave up; the
- * two-pass COO never waits and leaves it 0). Synchronous. */
+/* Reads a COO workspace's error word.  The two-pass COO never waits and
+ * leaves it 0; it stays for callers written against a waiting COO.
+ * Synchronous. */
 int mfp_workspace_error(const void *workspace, uint32_t *error);
+
+/* Load-ceiling probe (a measurement kernel; no counterpart in the reference).
+ * Issues an SpMV's memory operations over nnz (value, column) pairs without
+ * the rows: mode 0 streams values and column ids, mode 1 streams column ids
+ * and gathers x[col], mode 2 does both (every format's loads).  x_path: 0 the
+ * L1-cached read-only path, 1 L2 only (ld.global.cg), 2 read-only without L1
+ * allocation.  One partial sum per CTA goes to `out` (at least 148 * 8 =
+ * 1184 floats on a B200; fewer -> MFP_ERROR_INVALID_VALUE).  Arrays must be
+ * 16-byte aligned.  Its time on a matrix bounds every format's kernel time
+ * on that matrix from below. */
+int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values, const uint32_t *col_ids,
+                         const float *x, float *out, size_t out_len, void *stream);
 
 /* COO SpMV (float) that allocates nothing.  No counterpart in the reference:
  * it serves callers that may not allocate device memory themselves (hosts
  * that own every byte through their own pool or budget, or loops that cannot
  * take cudaMalloc's latency and implicit synchronisation).  Same arguments and
- * result as mfp_coo_spmv_f32 without the workspace, within the COO tolerance:
- * it runs the single-pass COO kernel (2048-element tiles; a tile that ends a
- * row begun in earlier tiles waits, bounded, for their published partial
- * sums), whose look-back scratch is a fixed 1 MiB array inside the library,
- * present on every device that loads it, so nnz is limited to 134,215,680
- * (larger -> MFP_ERROR_TOO_LARGE).
+ * the same result bits as mfp_coo_spmv_f32 without the workspace: it runs the
+ * same two-pass COO, whose workspace lives in a fixed 4 MiB array inside the
+ * library, present on every device that loads it, so nnz is limited to
+ * 44,739,072 (larger -> MFP_ERROR_TOO_LARGE, before any GPU work).
+ * The passes have no waits, so nothing can fail on the GPU after a successful
+ * launch; the array needs no clearing (every call rewrites what it reads).
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call clears the part of the array it uses with cudaMemsetAsync on
- * `stream`; all calls share the one array, so calls that overlap on the GPU
- * (different streams, or different host threads) race and must not be issued
+ * All calls share the one array, so calls that overlap on the GPU (different
+ * streams, or different host threads) race and must not be issued
  * concurrently. */
 int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
                              const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,

@@ -4,6 +4,7 @@
 #include "spmv_stream.cuh"
 #include "spmv_lowp.cuh"
 #include "mlp.cuh"
+#include "spmv_probe.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -593,18 +594,14 @@ cudaError_t launch_after(void (*k)(KArgs...), uint32_t grid, cudaStream_t s, Arg
   return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 
-// COO workspace: a 16-byte header (its error word stays 0: the two-pass COO
-// has no waits) and, per 256-element warp tile, the head and tail partial
-// sums (8 bytes each, FP64-sized), the flags and the tail row.
+// COO workspace: a 16-byte header (the first and last row holding elements;
+// its error word stays 0: the two-pass COO has no waits) and, per 256-element
+// warp tile, the head and tail partial sums (8 bytes each, FP64-sized), the
+// flags and the tail row.  Every call rewrites what it reads: no
+// initialisation.
 size_t coo_ws_bytes(uint32_t nnz) {
   const uint64_t wt = (nnz + (uint64_t)d::kWarpTile - 1) / d::kWarpTile;
   return sizeof(d::coo_ws_header) + wt * 24u;
-}
-// The single-pass look-back COO (the allocation-free entry point): a header and
-// one tile state per 2048 elements.
-size_t coo_lookback_ws_bytes(uint32_t nnz) {
-  const uint64_t tiles = (nnz + (uint64_t)d::kChunk - 1) / d::kChunk;
-  return sizeof(d::coo_ws_header) + tiles * sizeof(d::coo_tile_state<double>);
 }
 
 template <typename T, bool ACCUM = false>
@@ -618,6 +615,7 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
     return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_ws_bytes(nnz), ws_bytes);
   if (!aligned16(ws)) return fail(MFP_ERROR_INVALID_VALUE, "COO workspace must be 16-byte aligned");
   const uint32_t n_wt = ceil_div(nnz, d::kWarpTile);
+  auto *hdr = static_cast<d::coo_ws_header *>(ws);
   unsigned char *base = static_cast<unsigned char *>(ws) + sizeof(d::coo_ws_header);
   d::coo_carry<T> cw;
   cw.head = reinterpret_cast<T *>(base);
@@ -630,46 +628,25 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   // the accumulating warp pass (hybrid tail) follows the ELL launch of the same call
   cudaError_t e;
   if (ACCUM)
-    e = vec ? launch_after(d::coo_warp_kernel<T, true, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw)
-            : launch_after(d::coo_warp_kernel<T, false, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw);
+    e = vec ? launch_after(d::coo_warp_kernel<T, true, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr)
+            : launch_after(d::coo_warp_kernel<T, false, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr);
   else {
     if (vec)
-      d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+      d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
     else
-      d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw);
+      d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) return cuda_fail(e, "coo_warp_kernel launch");
-  if (n_wt > 1) {
-    e = launch_after(d::coo_fixup_kernel<T, ACCUM>, ceil_div(n_wt, d::kBlock), s, n_wt, cw, y);
+  // the fix-up pass finishes rows that cross tiles and, without ACCUM, zeroes
+  // the empty rows before the first and after the last row with elements
+  if (n_wt > 1 || !ACCUM) {
+    uint32_t fgrid = ceil_div(n_wt, d::kBlock);
+    if (!ACCUM) fgrid = std::max(fgrid, std::min(ceil_div(rows, d::kBlock * 8u), 148u * 4u));
+    e = launch_after(d::coo_fixup_kernel<T, ACCUM>, fgrid, s, n_wt, rows, cw, (const d::coo_ws_header *)hdr, y);
     if (e != cudaSuccess) return cuda_fail(e, "coo_fixup_kernel launch");
   }
   return ok();
-}
-
-// Single pass: 2048-element tiles taken by ticket; a tile that ends a row
-// begun in earlier tiles waits (bounded) for their published partial sums.
-template <typename T>
-int coo_lookback_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
-                      const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
-  if (rows == 0) return ok();
-  if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
-  if (nnz == 0) return fill<T>(rows, y, T(0), stream);
-  if (!data || !cols || !rids || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
-  if (!ws || ws_bytes < coo_lookback_ws_bytes(nnz))
-    return fail(MFP_ERROR_INVALID_VALUE, "COO workspace of %zu bytes needed, %zu given", coo_lookback_ws_bytes(nnz),
-                ws_bytes);
-  if (!aligned16(ws)) return fail(MFP_ERROR_INVALID_VALUE, "COO workspace must be 16-byte aligned");
-  auto *hdr = reinterpret_cast<d::coo_ws_header *>(ws);
-  auto *tiles = reinterpret_cast<d::coo_tile_state<T> *>(hdr + 1);
-  const uint32_t grid = ceil_div(nnz, d::kChunk);
-  const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
-  cudaStream_t s = as_stream(stream);
-  if (vec)
-    d::coo_kernel<T, true, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
-  else
-    d::coo_kernel<T, false, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, hdr, tiles);
-  return check_launch("coo_kernel launch");
 }
 
 template <typename T, bool VEC, bool XWIN, bool UNSORTED = false>
@@ -922,6 +899,38 @@ int mfp_lowp_spmv(int vt, uint32_t rows, uint32_t, uint32_t nnz, const uint32_t 
 int mfp_lowp_ell_spmv(int vt, uint32_t rows, uint32_t, uint32_t width, const uint16_t *q, const float *scale,
                       const uint32_t *cols, const uint16_t *off, const float *x, float *y, void *s) {
   return lowp_ell_spmv(vt, rows, width, q, scale, cols, off, x, y, s);
+}
+}  // extern "C"
+template <int MODE, int XPATH>
+int probe_launch(uint32_t nnz, const float *v, const uint32_t *c, const float *x, float *out, size_t out_len,
+                 cudaStream_t s) {
+  auto k = d::probe_loads_kernel<MODE, XPATH>;
+  uint32_t grid = 0;
+  int st = persistent_grid((const void *)k, d::kProbeBlock, 0, &grid);
+  if (st) return st;
+  if (out_len < grid) return fail(MFP_ERROR_INVALID_VALUE, "probe output needs %u floats, %zu given", grid, out_len);
+  k<<<grid, d::kProbeBlock, 0, s>>>(nnz, v, c, x, out);
+  return check_launch("probe_loads_kernel launch");
+}
+extern "C" {
+int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values, const uint32_t *col_ids,
+                         const float *x, float *out, size_t out_len, void *stream) {
+  if (mode < 0 || mode > 2 || x_path < 0 || x_path > 2) return fail(MFP_ERROR_INVALID_VALUE, "mode / x_path out of range");
+  if (nnz == 0) return ok();
+  if (!col_ids || !out || (mode != 1 && !values) || (mode != 0 && !x))
+    return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  if (!aligned16(col_ids) || (mode != 1 && !aligned16(values)))
+    return fail(MFP_ERROR_INVALID_VALUE, "the probe needs 16-byte-aligned arrays");
+  cudaStream_t s = as_stream(stream);
+  if (mode == 0) return probe_launch<0, 0>(nnz, values, col_ids, x, out, out_len, s);
+  if (mode == 1) {
+    if (x_path == 0) return probe_launch<1, 0>(nnz, values, col_ids, x, out, out_len, s);
+    if (x_path == 1) return probe_launch<1, 1>(nnz, values, col_ids, x, out, out_len, s);
+    return probe_launch<1, 2>(nnz, values, col_ids, x, out, out_len, s);
+  }
+  if (x_path == 0) return probe_launch<2, 0>(nnz, values, col_ids, x, out, out_len, s);
+  if (x_path == 1) return probe_launch<2, 1>(nnz, values, col_ids, x, out, out_len, s);
+  return probe_launch<2, 2>(nnz, values, col_ids, x, out, out_len, s);
 }
 int mfp_lowp_error(int device, int clear, uint32_t *error) {
   if (!error) return fail(MFP_ERROR_INVALID_VALUE, "null output");
@@ -1498,12 +1507,13 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
     out->algorithmic_bytes = m->nnz * 6 + (uint64_t)m->rows * 4 + ((uint64_t)m->rows + 1) * 4 +
                              (uint64_t)m->cols * 4 + (uint64_t)m->rows * 4;
   out->device_bytes = m->device_bytes;
-  // the two-pass COO launches its fix-up pass when there is more than one warp tile
-  auto coo_launches = [](uint64_t n) -> uint32_t { return n > d::kWarpTile ? 2u : 1u; };
+  // the two-pass COO: a warp pass, then the fix-up pass (always for plain COO,
+  // which zeroes leading and trailing empty rows there; for the hybrid's
+  // accumulating tail only when there is more than one warp tile)
   if (m->format == MFP_FORMAT_COO)
-    out->kernel_launches = coo_launches(m->nnz);
+    out->kernel_launches = m->nnz ? 2u : (m->rows ? 1u : 0u);
   else if (m->format == MFP_FORMAT_HYBRID)
-    out->kernel_launches = 1u + (m->coo_nnz ? coo_launches(m->coo_nnz) : 0u);
+    out->kernel_launches = 1u + (m->coo_nnz ? (m->coo_nnz > d::kWarpTile ? 2u : 1u) : 0u);
   else
     out->kernel_launches = 1u;
   return ok();
@@ -1955,10 +1965,13 @@ int mfp_batch_graph_launch(mfp_batch *b, const void *x, void *y, void *stream) {
 // Some callers cannot let a library call cudaMalloc: hosts that hand out all
 // device memory through their own pool or budget, and loops that cannot
 // afford cudaMalloc's latency and implicit synchronisation.  This entry point
-// keeps the COO look-back workspace in a fixed array that is part of the
-// library image instead.
+// runs the same two-pass COO as mfp_coo_spmv_f32 and keeps its workspace (the
+// per-warp-tile partial sums) in a fixed array that is part of the library
+// image instead.  The two passes have no waits, so there is no error state to
+// report after the launch; the workspace needs no clearing, since every call
+// rewrites what it reads.
 namespace {
-constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB on every device that loads the library
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB on every device that loads the library
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 std::mutex g_noalloc_mu;
 constexpr int kMaxDevices = 64;
@@ -1985,16 +1998,17 @@ int noalloc_scratch(void **out) {
 extern "C" int mfp_coo_spmv_f32_noalloc(uint32_t rows, uint32_t cols, uint32_t nnz, const float *data,
                                         const uint32_t *col_ids, const uint32_t *row_ids, const float *x, float *y,
                                         void *stream) {
-  const size_t need = coo_lookback_ws_bytes(nnz);
+  (void)cols;
+  const size_t need = coo_ws_bytes(nnz);
   if (need > kNoAllocScratchBytes)
     return fail(MFP_ERROR_TOO_LARGE,
                 "nnz %u needs %zu bytes of COO scratch; the fixed scratch holds %zu bytes (nnz <= %zu)", nnz, need,
-                kNoAllocScratchBytes,
-                (kNoAllocScratchBytes - sizeof(d::coo_ws_header)) / sizeof(d::coo_tile_state<double>) * d::kChunk);
+                kNoAllocScratchBytes, (kNoAllocScratchBytes - sizeof(d::coo_ws_header)) / 24u * d::kWarpTile);
+  if (rows == 0) return ok();
+  if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
+  if (nnz && (!data || !col_ids || !row_ids || !x)) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   void *ws = nullptr;
-  int st = noalloc_scratch(&ws);
+  const int st = noalloc_scratch(&ws);
   if (st) return st;
-  // the workspace must start zeroed; the previous call's contents are cleared on this stream
-  if (rows && nnz) CUDA_TRY(cudaMemsetAsync(ws, 0, need, as_stream(stream)), "cudaMemsetAsync(scratch)");
-  return coo_lookback_spmv<float>(rows, nnz, data, col_ids, row_ids, x, y, ws, need, stream);
+  return coo_spmv<float>(rows, nnz, data, col_ids, row_ids, x, y, ws, need, stream);
 }

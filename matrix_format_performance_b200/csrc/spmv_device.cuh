@@ -185,26 +185,10 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
   return s_warp[warp] + inc - v;
 }
 
-// Bounded spin on a flag written by an earlier CTA of the same launch.
-// Returns false (and the caller records an error) if the limit is reached.
-__device__ __forceinline__ bool wait_flag(const uint32_t *flag, uint32_t limit) {
-  for (uint32_t i = 0; i < limit; ++i) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-    if (v != 0u) return true;
-    __nanosleep(64);
-  }
-  return false;
-}
-
 // Programmatic dependent launch: waits until the preceding kernel of the
 // stream has completed and its writes are visible (a no-op when the launch did
 // not allow early start).  Hardware-managed; not a poll on memory.
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-__device__ __forceinline__ void store_release(uint32_t *flag, uint32_t v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
-}
 
 }  // namespace dev
 }  // namespace mfp

@@ -927,145 +927,18 @@ __global__ void __launch_bounds__(kBlock) ell_kernel(uint32_t n_rows, uint32_t w
   }
 }
 
-// ---------------------------------------------------------------------------
-// COO: tile = kChunk consecutive elements, taken in launch order from an
-// atomic ticket so every lower tile is already running.  Rows split between
-// tiles: the tile holding a row's last element (END) walks back over the
-// published partials of the earlier tiles (START / MIDDLE).  Waits are
-// bounded; on timeout the workspace error word is set.
-// ---------------------------------------------------------------------------
+// COO workspace header: the first and last row that hold elements (written
+// by the warp pass, read by the fix-up pass, which zeroes the empty rows
+// before and after them over its whole grid) and an error word that no COO
+// kernel sets (the two passes have no waits).
 struct coo_ws_header {
-  uint32_t ticket;
-  uint32_t done;
+  uint32_t first_row;
+  uint32_t last_row;
   uint32_t error;
   uint32_t pad;
 };
-template <typename T>
-struct coo_tile_state {
-  uint32_t flag;  // 1 when published
-  uint32_t kind;  // 1 START, 2 MIDDLE
-  T value;
-};
 
 constexpr uint32_t kNoRow = 0xffffffffu;
-constexpr uint32_t kWaitLimit = 1u << 22;  // ~0.3 s of 64 ns sleeps
-
-template <typename T>
-struct coo_smem {
-  seg_scan_smem<T> scan;
-  uint32_t tile;
-  T first_total, last_total;
-  uint32_t first_row, last_row;
-};
-
-// ACCUM: add each row's total to y instead of storing it, and leave rows
-// without elements untouched (the COO tail of the hybrid format, after the
-// ELL kernel has written every row).
-template <typename T, bool VEC, bool ACCUM = false>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64) coo_kernel(uint32_t n_rows, uint32_t nnz,
-                                                     const T *__restrict__ vals,
-                                                     const uint32_t *__restrict__ cols,
-                                                     const uint32_t *__restrict__ rows,
-                                                     const T *__restrict__ x, T *__restrict__ y,
-                                                     coo_ws_header *ws, coo_tile_state<T> *tiles) {
-  __shared__ coo_smem<T> sm;
-  const uint64_t pol = policy_evict_first();
-  if (threadIdx.x == 0) sm.tile = atomicAdd(&ws->ticket, 1u);
-  __syncthreads();
-  const uint32_t tile = sm.tile;
-  if (tile >= gridDim.x) {
-    // the workspace was not left zeroed (an interrupted launch): refuse the
-    // tile instead of reading past the arrays; the host sees the error word
-    if (threadIdx.x == 0) {
-      atomicOr(&ws->error, 2u);
-      const uint32_t d = atomicAdd(&ws->done, 1u);
-      if (d == gridDim.x - 1) {
-        ws->ticket = 0u;
-        ws->done = 0u;
-      }
-    }
-    return;
-  }
-  const uint32_t c0 = tile * (uint32_t)kChunk;
-  const uint32_t c1 = min(nnz, c0 + (uint32_t)kChunk);
-  const uint32_t p = c0 > 0 ? rows[c0 - 1] : kNoRow;
-  const uint32_t nx = c1 < nnz ? rows[c1] : kNoRow;
-  // c0 is a multiple of kChunk: thread t owns elements c0 + 8 t .. c0 + 8 t + 7
-  T pr[kEpt];
-  uint32_t rw[kEpt], i0 = 0;
-  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + threadIdx.x * kEpt, c0, c1, pr,
-                                              rw, i0, pol);
-  const uint32_t rf = __ldg(rows + c0), rl = __ldg(rows + c1 - 1u);
-  // empty rows before the first row of this tile (after the previous tile's last)
-  if (!ACCUM) {
-    const uint32_t lo = (p == kNoRow) ? 0u : p + 1u;
-    for (uint32_t r = lo + threadIdx.x; r < rf && r < n_rows; r += kBlock) y[r] = T(0);
-    if (c1 == nnz)
-      for (uint32_t r = rl + 1u + threadIdx.x; r < n_rows; r += kBlock) y[r] = T(0);
-  }
-  auto emit = [&](uint32_t row, T total, bool is_first, bool is_last) {
-    const bool cont_prev = is_first && row == p;
-    const bool cont_next = is_last && row == nx;
-    if (!cont_prev && !cont_next) {
-      if (row < n_rows) y[row] = ACCUM ? add_rn(y[row], total) : total;
-      return;
-    }
-    if (is_first) sm.first_total = total;
-    if (is_last) sm.last_total = total;
-  };
-  auto gap = [&](uint32_t lo, uint32_t hi) {
-    if (!ACCUM)
-      for (uint32_t r = lo; r < hi && r < n_rows; ++r) y[r] = T(0);
-  };
-  block_segmented_reduce_regs<T>(pr, rw, cnt, i0, c0, c1, rows, emit, gap, sm.scan);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const bool first_prev = (rf == p), last_next = (rl == nx);
-    if (rf == rl) {
-      const T v = sm.first_total;
-      if (first_prev && last_next) {
-        tiles[tile].value = v;
-        tiles[tile].kind = 2u;
-        store_release(&tiles[tile].flag, 1u);
-      } else if (!first_prev && last_next) {
-        tiles[tile].value = v;
-        tiles[tile].kind = 1u;
-        store_release(&tiles[tile].flag, 1u);
-      }
-    } else if (last_next) {
-      tiles[tile].value = sm.last_total;
-      tiles[tile].kind = 1u;
-      store_release(&tiles[tile].flag, 1u);
-    }
-    if (first_prev && !(rf == rl && last_next)) {
-      // this tile ends row rf: walk back over earlier tiles
-      T sum = T(0);
-      uint32_t c = tile;
-      bool ok = true;
-      while (c > 0) {
-        --c;
-        if (!wait_flag(&tiles[c].flag, kWaitLimit)) {
-          ok = false;
-          break;
-        }
-        const T v = __ldcg(&tiles[c].value);
-        const uint32_t kind = __ldcg(&tiles[c].kind);
-        tiles[c].flag = 0u;  // consumed
-        sum = add_rn(v, sum);
-        if (kind != 2u) break;
-      }
-      if (!ok) atomicOr(&ws->error, 1u);
-      if (rf < n_rows) y[rf] = ACCUM ? add_rn(y[rf], add_rn(sum, sm.first_total)) : add_rn(sum, sm.first_total);
-    }
-    // the tile state this thread wrote is ordered by the release stores; the
-    // counters are reset by the last CTA and read again only by the next launch
-    const uint32_t d = atomicAdd(&ws->done, 1u);
-    if (d == gridDim.x - 1) {
-      ws->ticket = 0u;
-      ws->done = 0u;
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // COO in two passes (the default COO and hybrid-tail path).
@@ -1089,9 +962,10 @@ struct coo_carry {
   uint32_t *flags, *tail_row;
 };
 
+// Row ids at or above n_rows (invalid input) are dropped, never written.
 template <typename T, bool ACCUM>
-__device__ __forceinline__ void coo_put(T *y, uint32_t row, T v) {
-  y[row] = ACCUM ? add_rn(y[row], v) : v;
+__device__ __forceinline__ void coo_put(T *y, uint32_t n_rows, uint32_t row, T v) {
+  if (row < n_rows) y[row] = ACCUM ? add_rn(y[row], v) : v;
 }
 
 // The reduction of one warp tile [c0, c1) of nnz elements, the lane's cnt
@@ -1101,7 +975,7 @@ template <typename T, bool ACCUM>
 __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint32_t c1, uint32_t nnz,
                                                  uint32_t n_rows, const T (&pr)[kEpt], const uint32_t (&rw)[kEpt],
                                                  uint32_t cnt, uint32_t prv, uint32_t nxt, T *__restrict__ y,
-                                                 const coo_carry<T> &cw) {
+                                                 const coo_carry<T> &cw, coo_ws_header *hdr) {
   const uint32_t lane = threadIdx.x & 31u;
   const bool active = cnt > 0;
   const uint32_t last_lane = (c1 - c0 - 1u) / kEpt;
@@ -1120,9 +994,9 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
           acc = add_rn(acc, pr[k]);
         } else {
           if (first) sf = acc;
-          else coo_put<T, ACCUM>(y, cur, acc);
+          else coo_put<T, ACCUM>(y, n_rows, cur, acc);
           if (!ACCUM)
-            for (uint32_t r = cur + 1u; r < rw[k]; ++r) y[r] = T(0);
+            for (uint32_t r = cur + 1u; r < rw[k] && r < n_rows; ++r) y[r] = T(0);
           first = false;
           cur = rw[k];
           acc = pr[k];
@@ -1159,23 +1033,28 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
   // rows are sorted: the first run reaches back beyond the tile exactly when
   // its row is the row before the tile
   const bool from_prev = rf == prv;
-  // empty rows before this lane's first row
+  // empty rows before this lane's first row; those before the matrix's first
+  // row are left to the fix-up pass, which spreads them over its grid
   if (!ACCUM) {
-    const uint32_t lo = lane == 0 ? (prv == kNoRow ? 0u : prv + 1u) : prev_last + 1u;
-    for (uint32_t r = lo; r < rf; ++r) y[r] = T(0);
+    if (lane == 0 && prv == kNoRow) {
+      hdr->first_row = rf;
+    } else {
+      const uint32_t lo = lane == 0 ? prv + 1u : prev_last + 1u;
+      for (uint32_t r = lo; r < rf && r < n_rows; ++r) y[r] = T(0);
+    }
   }
   const uint32_t after = lane < last_lane ? next_first : nxt;  // row of the element after this lane
   if (!single) {
     // first run ends inside the lane
     if (from_prev) cw.head[wt] = ftot;
-    else coo_put<T, ACCUM>(y, rf, ftot);
+    else coo_put<T, ACCUM>(y, n_rows, rf, ftot);
   }
   // last run (the first run too when single)
   const T ltot = single ? ftot : sl;
   const bool l_from_prev = single && from_prev;
   if (after != rl) {
     if (l_from_prev) cw.head[wt] = ltot;
-    else coo_put<T, ACCUM>(y, rl, ltot);
+    else coo_put<T, ACCUM>(y, n_rows, rl, ltot);
   } else if (lane == last_lane) {
     // the tail row continues into the next tile
     cw.tail[wt] = ltot;
@@ -1188,8 +1067,7 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
     if (rl == nxt) f |= kTailCont;          // its last row goes on in the next tile
     if (tile_first == rl) f |= kOneRow;
     cw.flags[wt] = f;
-    if (!ACCUM && c1 == nnz)
-      for (uint32_t r = rl + 1u; r < n_rows; ++r) y[r] = T(0);
+    if (!ACCUM && c1 == nnz) hdr->last_row = rl;  // the fix-up pass zeroes the rows after it
   }
 }
 
@@ -1197,7 +1075,7 @@ template <typename T, bool VEC, bool ACCUM>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
-                    coo_carry<T> cw) {
+                    coo_carry<T> cw, coo_ws_header *hdr) {
   if (ACCUM) griddep_wait();  // y holds the ELL part written by the preceding launch
   const uint64_t pol = policy_evict_first();
   const uint32_t lane = threadIdx.x & 31u;
@@ -1210,21 +1088,33 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
                                               i0, pol);
   const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
   const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
-  warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw);
+  warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw, hdr);
 }
 
 // Pass 2: the row starting in tile w that continues past it.  The tiles that
 // follow are read 16 at a time (their loads in flight together) and walked in
 // order in registers: a row of 50,000 elements spans 195 tiles, and one
 // dependent load per tile would make it the launch's critical path.
+// Without ACCUM the whole grid then zeroes the rows before the first row and
+// after the last row that hold elements (grid-stride; the grid may be larger
+// than one thread per tile for that).
 #ifndef MFP_FIXUP_BATCH
 #define MFP_FIXUP_BATCH 16
 #endif
 template <typename T, bool ACCUM>
-__global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, coo_carry<T> cw, T *__restrict__ y) {
+__global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, uint32_t n_rows, coo_carry<T> cw,
+                                                           const coo_ws_header *hdr, T *__restrict__ y) {
   constexpr uint32_t B = MFP_FIXUP_BATCH;
   griddep_wait();  // the warp pass's partial sums and rows of y
   const uint32_t w = blockIdx.x * kBlock + threadIdx.x;
+  if (!ACCUM) {
+    const uint32_t first = min(hdr->first_row, n_rows);
+    const uint32_t last = hdr->last_row;
+    const uint32_t step = gridDim.x * kBlock;
+    for (uint32_t r = w; r < first; r += step) y[r] = T(0);
+    if (last < n_rows)
+      for (uint32_t r = last + 1u + w; r < n_rows; r += step) y[r] = T(0);
+  }
   if (w >= n_tiles) return;
   const uint32_t f = cw.flags[w];
   if (!(f & kTailCont) || ((f & kOneRow) && (f & kHeadCont))) return;
@@ -1254,7 +1144,7 @@ __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, coo
       break;
     }
   }
-  coo_put<T, ACCUM>(y, row, acc);
+  coo_put<T, ACCUM>(y, n_rows, row, acc);
 }
 
 // ---------------------------------------------------------------------------

@@ -5,6 +5,8 @@ rows it owns and y is the concatenation of the ranks' slices.
 - row_partition   contiguous row ranges balanced by nonzeros plus rows (a
                   prefix sum over row_ptr and a binary search per boundary)
 - shard_csr       the CSR of one rank's rows (columns stay global)
+- rank_shard      row_partition + shard_csr for one rank (what bench.py's
+                  ranks run)
 - assign_matrices whole matrices of a batch to ranks, balanced by bytes
                   (largest first onto the least-loaded rank)
 An x distributed by rows would first need one all-gather of the x slices;
@@ -34,6 +36,15 @@ def shard_csr(m: csr_matrix_class, lo: int, hi: int) -> csr_matrix_class:
     e0, e1 = rp[lo], rp[hi]
     return csr_matrix_class.from_arrays(hi - lo, m.cols, (rp[lo:hi + 1] - e0).astype(np.uint32),
                                         m.columns[e0:e1], m.data[e0:e1], m.dtype)
+
+
+def rank_shard(m: csr_matrix_class, rank: int, world: int) -> tuple[csr_matrix_class, int, int]:
+    """The rows one rank runs in a strong-scaling SpMV of m (x replicated):
+    (its CSR shard, first row, one past its last row).  bench.py's ranks and
+    the multi-process tests both take their rows from here."""
+    b = row_partition(m.row_ptr, world)
+    lo, hi = int(b[rank]), int(b[rank + 1])
+    return shard_csr(m, lo, hi), lo, hi
 
 
 def matrix_bytes(m: csr_matrix_class) -> int:

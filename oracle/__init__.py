@@ -13,4 +13,4 @@ The restatement is pinned to the reference by tests/test_oracle.py (against
 _ref when present, and always against the committed fixtures in
 tests/golden/, which _ref produced).
 """
-from .oracle import (HERE, Oracle, RefLib, build, load_oracle, load_ref)  # noqa: F401
+from .oracle import (HERE, Oracle, RefLib, build, load_oracle, load_ref, load_synth, synth_power_law)  # noqa: F401

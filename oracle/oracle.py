@@ -11,7 +11,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libmfp_ref.so"
-REFERENCE_SRC = Path(os.environ.get("MFP_REFERENCE_SRC", "/root/reference"))
+SYNTH_SO = HERE / "libmfp_synth.so"
+# the reference checkout: MFP_REFERENCE_SRC, else the default of oracle/Makefile
+REFERENCE_SRC = os.environ.get("MFP_REFERENCE_SRC")
 
 vp, u32, u64, i32, i64, f64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_longlong, C.c_double
 
@@ -25,13 +27,27 @@ def _p(a):
     return C.c_void_p(a.ctypes.data)
 
 
+def _ref_dir() -> Path | None:
+    """The reference checkout the recipe would compile, or None when absent."""
+    if REFERENCE_SRC:
+        d = Path(REFERENCE_SRC)
+    else:
+        r = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], capture_output=True, text=True)
+        d = Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else None
+    return d if d is not None and (d / "common" / "matrix_converter.cpp").exists() else None
+
+
 def build(ref: bool | None = None) -> None:
-    """Builds liboracle.so, and _ref/libmfp_ref.so when the reference sources exist."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    """Builds liboracle.so and libmfp_synth.so, and _ref/libmfp_ref.so when the
+    reference sources exist (MFP_REFERENCE_SRC, else oracle/Makefile's REF)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so", "libmfp_synth.so"], check=True)
+    src = _ref_dir()
     if ref is None:
-        ref = (REFERENCE_SRC / "common" / "matrix_converter.cpp").exists()
+        ref = src is not None
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_SRC}"], check=True)
+        if src is None:
+            raise FileNotFoundError("reference sources not found: set MFP_REFERENCE_SRC")
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={src}"], check=True)
 
 
 class Oracle:
@@ -300,3 +316,38 @@ def load_ref() -> RefLib | None:
     if _ref is None and REF_SO.exists():
         _ref = RefLib()
     return _ref
+
+
+_synth = None
+
+
+def load_synth() -> C.CDLL:
+    """The seeded matrix generator alone (libmfp_synth.so: the engine's
+    generator source built without the engine), so the benchmark's reference
+    arm maps no engine library."""
+    global _synth
+    if _synth is None:
+        if not SYNTH_SO.exists():
+            build(ref=False)
+        _synth = C.CDLL(str(SYNTH_SO))
+        _synth.mfp_synth_csr.restype = i32
+        _synth.mfp_synth_csr.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    return _synth
+
+
+def synth_power_law(rows: int, seed: int, cols: int, alpha: float = 2.0, k_lo: int = 1, k_hi: int = 50_000):
+    """(rows, cols, row_ptr, columns, values float64) of the seeded power-law
+    matrix: the same arrays as the engine's synth.power_law."""
+    from matrix_format_performance_b200._capi import SynthParams  # a ctypes struct; loads no library
+    lib = load_synth()
+    p = SynthParams(1, seed, rows, cols, alpha, k_lo, k_hi, 0)
+    r, c, n = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    if lib.mfp_synth_csr(C.byref(p), C.byref(r), C.byref(c), C.byref(n), None, None, None):
+        raise RuntimeError("mfp_synth_csr (size query) failed")
+    rp = np.empty(r.value + 1, np.uint32)
+    ci = np.empty(max(1, n.value), np.uint32)
+    va = np.empty(max(1, n.value), np.float64)
+    if lib.mfp_synth_csr(C.byref(p), C.byref(r), C.byref(c), C.byref(n), _p(rp), C.c_void_p(ci.ctypes.data),
+                         C.c_void_p(va.ctypes.data)):
+        raise RuntimeError("mfp_synth_csr failed")
+    return r.value, c.value, rp, ci[:n.value], va[:n.value]

@@ -1,11 +1,12 @@
 """The multi-GPU sharding logic on world_size-2 gloo process groups (CPU).
 
-Each rank takes its row shard of a power-law matrix (partition.row_partition),
-computes its y slice with the oracle, and the all-gathered slices must equal
-the single-process product bit for bit; the shards' nonzeros are balanced.
-For batches, every matrix is assigned to exactly one rank and the ranks'
-bytes are balanced.  No GPU: this is the host-side partitioning that
-bench.py's ranks use, exercised with real process groups.
+Each rank takes its row shard of a power-law matrix with partition.rank_shard
+(the call bench.py's ranks make for strong scaling), computes its y slice
+with the oracle (the engine's kernels need a GPU), and the all-gathered slices
+must equal the single-process product bit for bit; the shards' nonzeros are
+balanced.  For batches, every matrix is assigned to exactly one rank and the
+ranks' bytes are balanced.  No GPU: the host-side sharding exercised with real
+process groups.
 """
 import os
 import socket
@@ -26,15 +27,15 @@ def _rows_worker(rank, world, port, q):
     import torch
 
     from matrix_format_performance_b200 import synth
-    from matrix_format_performance_b200.partition import row_partition, shard_csr
+    from matrix_format_performance_b200.partition import rank_shard
     from oracle import load_oracle
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         m = synth.power_law(rows=60_000, seed=5).astype(np.float32)
         x = synth.vector(2, m.cols).astype(np.float32)
-        b = row_partition(m.row_ptr, world)
-        s = shard_csr(m, int(b[rank]), int(b[rank + 1]))
+        s, lo, hi = rank_shard(m, rank, world)
+        assert s.rows == hi - lo
         orc = load_oracle()
         y_local = orc.csr_spmv(s.rows, s.row_ptr, s.columns, s.data, x).astype(np.float32)
         sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]

@@ -211,6 +211,36 @@ def test_coo_tiles_sharing_rows(oracle_lib):
     assert np.array_equal(ys[0], ys[2])
 
 
+@pytest.mark.parametrize("nnz_valid", [100, 5_000, 70_000])
+def test_coo_drops_row_ids_beyond_rows(oracle_lib, nnz_valid):
+    """Row ids >= rows are dropped: y past `rows` (here a guard region of the
+    same allocation, which the ids point into) is never written."""
+    rng = np.random.default_rng(nnz_valid)
+    rows, cols, guard = 3_000, 500, 64
+    r = np.sort(rng.integers(0, rows, size=nnz_valid)).astype(np.uint32)
+    r = np.concatenate([r, np.array([rows, rows + 3, rows + 3, rows + 40], np.uint32)])
+    c = rng.integers(0, cols, size=r.size).astype(np.uint32)
+    v = rng.uniform(-1, 1, size=r.size).astype(np.float32)
+    x = rng.uniform(-1, 1, size=cols).astype(np.float32)
+    rp = np.zeros(rows + 1, np.int64)
+    np.add.at(rp, r[:nnz_valid].astype(np.int64) + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    ys, ab = oracle_lib.csr_spmv_exact(rows, rp, c[:nnz_valid], v[:nnz_valid], x)
+    d_v, d_c, d_r, d_x = (torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()
+                          for a in (v, c, r, x))
+    y = torch.full((rows + guard,), 7.0, device="cuda")
+    nbytes = C.c_size_t()
+    call("mfp_coo_workspace_bytes", rows, r.size, C.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    call("mfp_coo_spmv_f32", rows, cols, r.size, *(C.c_void_p(t.data_ptr()) for t in (d_v, d_c, d_r, d_x, y, ws)),
+         nbytes.value, stream)
+    torch.cuda.synchronize()
+    got = y.cpu().numpy()
+    assert np.all(got[rows:] == 7.0)
+    assert np.all(np.abs(got[:rows].astype(np.float64) - ys) <= 1e-5 * ab)
+
+
 def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
     m = syn("power_law_300k").astype(np.float32)
     x = synth.vector(4, m.cols).astype(np.float32)
