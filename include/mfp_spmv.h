@@ -288,7 +288,9 @@ int mfp_workspace_error(const void *workspace, uint32_t *error);
 /* Load-ceiling probe (a measurement kernel; no counterpart in the reference).
  * Issues an SpMV's memory operations over nnz (value, column) pairs without
  * the rows: mode 0 streams values and column ids, mode 1 streams column ids
- * and gathers x[col], mode 2 does both (every format's loads).  x_path: 0 the
+ * and gathers x[col], mode 2 does both (every format's loads), mode 3 is
+ * mode 1 with every gather folded into x[0, 4096) (held in L1; x needs at
+ * least 4096 entries).  x_path: 0 the
  * L1-cached read-only path, 1 L2 only (ld.global.cg), 2 read-only without L1
  * allocation.  One partial sum per CTA goes to `out` (at least 148 * 8 =
  * 1184 floats on a B200; fewer -> MFP_ERROR_INVALID_VALUE).  Arrays must be
@@ -296,6 +298,13 @@ int mfp_workspace_error(const void *workspace, uint32_t *error);
  * on that matrix from below. */
 int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values, const uint32_t *col_ids,
                          const float *x, float *out, size_t out_len, void *stream);
+/* The same probe with the x gathers done by TMA (cp.async.bulk.tensor
+ * tile::gather4: four 16-byte rows of x per instruction into shared memory),
+ * mode 4 all of them, mode 5 half (the other half by ld.global.nc).  x has
+ * n_x entries (n_x % 4 == 0, 16-byte aligned); the last nnz % 256 elements
+ * are not visited.  A CTA whose bounded wait gave up writes NaN to out. */
+int mfp_probe_spmv_gather4(int mode, uint32_t nnz, uint32_t n_x, const uint32_t *col_ids, const float *x, float *out,
+                           size_t out_len, void *stream);
 
 /* COO SpMV (float) that allocates nothing.  No counterpart in the reference:
  * it serves callers that may not allocate device memory themselves (hosts
@@ -385,7 +394,10 @@ int mfp_lowp_deltas(uint32_t nnz, const uint32_t *columns, uint16_t *delta, uint
  * (16-bit) is given, the other null.  With q, the indices and row_ptr
  * 16-byte aligned the launch is the pipelined kernel (TMA bulk copies into
  * shared-memory stages); otherwise a row-block kernel with plain loads.  Both
- * are within FP32 rounding of each other (their sum orders differ). */
+ * are within FP32 rounding of each other (their sum orders differ).  The
+ * pipelined kernel sums each row in one thread: for matrices with rows longer
+ * than 1,024 elements use a handle (mfp_matrix_create_lowp), which sends them
+ * to the row-block kernel, where a warp shares each row longer than 128. */
 int mfp_lowp_spmv(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row_ptr,
                   const uint16_t *q, const float *scale, const uint32_t *columns, const uint16_t *delta,
                   const uint32_t *base, const float *x, float *y, void *stream);

@@ -105,6 +105,7 @@ _PROTOS = {
     "mfp_lowp_spmv": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp],
     "mfp_lowp_error": [i32, i32, P_u32],
     "mfp_probe_spmv_loads": [i32, i32, u32, vp, vp, vp, vp, C.c_size_t, vp],
+    "mfp_probe_spmv_gather4": [i32, u32, u32, vp, vp, vp, C.c_size_t, vp],
     "mfp_lowp_ell_from_csr": [i32, i32, u32, u32, vp, vp, vp, u32, vp, vp, vp],
     "mfp_lowp_ell_spmv": [i32, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp],
     "mfp_matrix_create_lowp_ell": [i32, i32, u32, u32, u32, vp, vp, vp, C.POINTER(vp)],

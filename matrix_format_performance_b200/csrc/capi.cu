@@ -724,9 +724,13 @@ int lowp_tma_launch(const d::lowp_args<VT, D16> &A, uint32_t nnz, cudaStream_t s
   return check_launch("lowp_tma_kernel launch");
 }
 
+// long_rows: the matrix has rows longer than kLowpTmaMaxRow elements; they go
+// to the row-block kernel, whose warps share long rows (the pipelined kernel
+// sums each row in one thread).  Handles know it; the raw entry point does not.
+constexpr uint32_t kLowpTmaMaxRow = 1024;
 int lowp_spmv(int vt, uint32_t rows, uint32_t nnz, const uint32_t *rp, const uint16_t *q, const float *scale,
               const uint32_t *cols, const uint16_t *delta, const uint32_t *base, const float *x, float *y,
-              void *stream) {
+              void *stream, bool long_rows = false) {
   if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
   if (rows == 0) return ok();
   if (rows > 0xffffff00u) return fail(MFP_ERROR_TOO_LARGE, "too many rows");
@@ -736,7 +740,7 @@ int lowp_spmv(int vt, uint32_t rows, uint32_t nnz, const uint32_t *rp, const uin
   const bool vec = aligned16(q) && (d16 ? aligned16(delta) : aligned16(cols));
   cudaStream_t s = as_stream(stream);
   // TMA bulk copies need 16-byte-aligned sources: values, indices and row_ptr
-  if (MFP_LOWP_TMA && nnz && vec && aligned16(rp)) {
+  if (MFP_LOWP_TMA && nnz && vec && aligned16(rp) && !long_rows) {
     if (vt == MFP_BF16)
       return d16 ? lowp_tma_launch<2, true>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s)
                  : lowp_tma_launch<2, false>({rows, rp, q, scale, cols, delta, base, x, y}, nnz, s);
@@ -912,14 +916,68 @@ int probe_launch(uint32_t nnz, const float *v, const uint32_t *c, const float *x
   k<<<grid, d::kProbeBlock, 0, s>>>(nnz, v, c, x, out);
   return check_launch("probe_loads_kernel launch");
 }
+// x as a 2-D tensor of n/4 rows of 4 floats (16-byte rows; x 16-byte aligned,
+// n a multiple of 4), box one row high: the map tile::gather4 needs.
+int x_rows_map(const float *x, uint32_t n, CUtensorMap *map) {
+  using encode_fn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static encode_fn encode = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!encode) {
+      void *fn = nullptr;
+      cudaDriverEntryPointQueryResult q{};
+      const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+      if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return fail(MFP_ERROR_CUDA, "cuTensorMapEncodeTiled entry point not found");
+      encode = reinterpret_cast<encode_fn>(fn);
+    }
+  }
+  if (!aligned16(x) || n % 4 != 0 || n < 4) return fail(MFP_ERROR_INVALID_VALUE, "x must be 16-byte aligned with n %% 4 == 0");
+  const cuuint64_t dims[2] = {4, n / 4};
+  const cuuint64_t strides[1] = {16};
+  const cuuint32_t box[2] = {4, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(x), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MFP_ERROR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return ok();
+}
+template <int MODE>
+int probe_g4_launch(uint32_t nnz, uint32_t n_x, const uint32_t *c, const float *x, float *out, size_t out_len,
+                    cudaStream_t s) {
+  CUtensorMap map;
+  int st = x_rows_map(x, n_x, &map);
+  if (st) return st;
+  auto k = d::probe_gather4_kernel<MODE>;
+  if ((st = ensure_dyn_smem((const void *)k, d::kG4DynBytes, "probe_gather4_kernel"))) return st;
+  uint32_t grid = 0;
+  if ((st = persistent_grid((const void *)k, d::kG4Warps * 32, d::kG4DynBytes, &grid))) return st;
+  if (out_len < grid) return fail(MFP_ERROR_INVALID_VALUE, "probe output needs %u floats, %zu given", grid, out_len);
+  k<<<grid, d::kG4Warps * 32, d::kG4DynBytes, s>>>(nnz, c, x, map, out);
+  return check_launch("probe_gather4_kernel launch");
+}
 extern "C" {
+int mfp_probe_spmv_gather4(int mode, uint32_t nnz, uint32_t n_x, const uint32_t *col_ids, const float *x, float *out,
+                           size_t out_len, void *stream) {
+  if (mode != 4 && mode != 5) return fail(MFP_ERROR_INVALID_VALUE, "mode must be 4 or 5");
+  if (nnz == 0) return ok();
+  if (!col_ids || !x || !out) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
+  if (!aligned16(col_ids)) return fail(MFP_ERROR_INVALID_VALUE, "the probe needs 16-byte-aligned arrays");
+  cudaStream_t s = as_stream(stream);
+  return mode == 4 ? probe_g4_launch<4>(nnz, n_x, col_ids, x, out, out_len, s)
+                   : probe_g4_launch<5>(nnz, n_x, col_ids, x, out, out_len, s);
+}
 int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values, const uint32_t *col_ids,
                          const float *x, float *out, size_t out_len, void *stream) {
-  if (mode < 0 || mode > 2 || x_path < 0 || x_path > 2) return fail(MFP_ERROR_INVALID_VALUE, "mode / x_path out of range");
+  if (mode < 0 || mode > 3 || x_path < 0 || x_path > 2) return fail(MFP_ERROR_INVALID_VALUE, "mode / x_path out of range");
   if (nnz == 0) return ok();
-  if (!col_ids || !out || (mode != 1 && !values) || (mode != 0 && !x))
+  if (!col_ids || !out || ((mode == 0 || mode == 2) && !values) || (mode != 0 && !x))
     return fail(MFP_ERROR_INVALID_VALUE, "null device array");
-  if (!aligned16(col_ids) || (mode != 1 && !aligned16(values)))
+  if (!aligned16(col_ids) || ((mode == 0 || mode == 2) && !aligned16(values)))
     return fail(MFP_ERROR_INVALID_VALUE, "the probe needs 16-byte-aligned arrays");
   cudaStream_t s = as_stream(stream);
   if (mode == 0) return probe_launch<0, 0>(nnz, values, col_ids, x, out, out_len, s);
@@ -928,6 +986,7 @@ int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values
     if (x_path == 1) return probe_launch<1, 1>(nnz, values, col_ids, x, out, out_len, s);
     return probe_launch<1, 2>(nnz, values, col_ids, x, out, out_len, s);
   }
+  if (mode == 3) return probe_launch<3, 0>(nnz, values, col_ids, x, out, out_len, s);
   if (x_path == 0) return probe_launch<2, 0>(nnz, values, col_ids, x, out, out_len, s);
   if (x_path == 1) return probe_launch<2, 1>(nnz, values, col_ids, x, out, out_len, s);
   return probe_launch<2, 2>(nnz, values, col_ids, x, out, out_len, s);
@@ -995,6 +1054,7 @@ struct mfp_matrix {
   uint16_t *delta = nullptr;          // 16-bit column deltas (else cols_a)
   uint32_t *base = nullptr;
   bool rows_unsorted = false;         // SCOO in the sort_cols layout
+  bool long_rows = false;             // reduced-precision CSR: a row longer than kLowpTmaMaxRow
 };
 
 namespace {
@@ -1440,6 +1500,7 @@ int mfp_matrix_create_lowp(int vt, int index16, uint32_t rows, uint32_t cols, ui
   m->rows = rows;
   m->cols = cols;
   m->nnz = nnz;
+  for (uint32_t r = 0; r < rows && !m->long_rows; ++r) m->long_rows = rp[r + 1] - rp[r] > kLowpTmaMaxRow;
   m->format_bytes = (uint64_t)nnz * (index16 ? 4 : 6) + (uint64_t)bs.size() * 4 + (uint64_t)rows * 4 +
                     ((uint64_t)rows + 1) * 4 + (uint64_t)cols * 4 + (uint64_t)rows * 4;
   if ((st = track_upload(m, &m->rows_a, rp, (size_t)rows + 1)) || (st = track_upload(m, &m->scale, sc.data(), sc.size())) ||
@@ -1565,7 +1626,8 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                            m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);
     case MFP_FORMAT_CSR_LOWP:
       return lowp_spmv(m->lowp_vt, m->rows, (uint32_t)m->nnz, m->rows_a, (const uint16_t *)m->vals, m->scale,
-                       m->delta ? nullptr : m->cols_a, m->delta, m->base, (const float *)x, (float *)y, stream);
+                       m->delta ? nullptr : m->cols_a, m->delta, m->base, (const float *)x, (float *)y, stream,
+                       m->long_rows);
     default:
       return fail(MFP_ERROR_INVALID_VALUE, "unknown format %d", m->format);
   }

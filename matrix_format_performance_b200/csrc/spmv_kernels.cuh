@@ -1115,19 +1115,22 @@ __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, uin
     if (last < n_rows)
       for (uint32_t r = last + 1u + w; r < n_rows; r += step) y[r] = T(0);
   }
-  if (w >= n_tiles) return;
-  const uint32_t f = cw.flags[w];
-  if (!(f & kTailCont) || ((f & kOneRow) && (f & kHeadCont))) return;
-  T acc = cw.tail[w];
-  const uint32_t row = cw.tail_row[w];
-  // the row ends in the first following tile that does not hold only this row
-  // and continue; the last tile never continues, so that tile exists
-  for (uint32_t k0 = w + 1u; k0 < n_tiles; k0 += B) {
+  const uint32_t f = w < n_tiles ? cw.flags[w] : 0u;
+  // this thread's tile starts a row that goes on into the next tile
+  const bool chain = (f & kTailCont) && !((f & kOneRow) && (f & kHeadCont));
+  T acc = T(0);
+  uint32_t row = 0, next = 0;  // next: the first tile not examined yet
+  bool more = false;           // the row goes on beyond the first batch
+  if (chain) {
+    acc = cw.tail[w];
+    row = cw.tail_row[w];
+    // the row ends in the first following tile that does not hold only this
+    // row and continue; the last tile never continues, so that tile exists
     uint32_t g[B];
     T t[B];
 #pragma unroll
     for (uint32_t j = 0; j < B; ++j) {
-      const uint32_t k = k0 + j;
+      const uint32_t k = w + 1u + j;
       g[j] = k < n_tiles ? cw.flags[k] : 0u;
       t[j] = k < n_tiles ? cw.tail[k] : T(0);
     }
@@ -1139,12 +1142,50 @@ __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, uin
         else end = j;
       }
     }
-    if (end < B) {
-      acc = add_rn(acc, cw.head[k0 + end]);
-      break;
-    }
+    if (end < B) acc = add_rn(acc, cw.head[w + 1u + end]);
+    else more = true, next = w + 1u + B;
   }
-  coo_put<T, ACCUM>(y, n_rows, row, acc);
+  // Rows longer than the first batch (a few per matrix, up to hundreds of
+  // tiles): the whole warp walks them, 256 tiles per round (lane l holds
+  // tiles base + 8 l .. base + 8 l + 7, so lane order is tile order); the
+  // round's tails are summed by a fixed shuffle tree.
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t todo = __ballot_sync(0xffffffffu, more); todo; todo &= todo - 1u) {
+    const uint32_t src = __ffs(todo) - 1u;
+    uint32_t base = __shfl_sync(0xffffffffu, next, src);
+    T racc = T(0);  // the sum of the rounds so far (same value in every lane)
+    uint32_t end_tile = 0;
+    for (;;) {
+      uint32_t g[8];
+      T t[8];
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j) {
+        const uint32_t k = base + 8u * lane + j;
+        g[j] = k < n_tiles ? cw.flags[k] : 0u;
+        t[j] = k < n_tiles ? cw.tail[k] : T(0);
+      }
+      uint32_t first_np = 8;  // first tile of this lane that ends the row
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j)
+        if (first_np == 8 && !((g[j] & kOneRow) && (g[j] & kTailCont))) first_np = j;
+      const uint32_t np = __ballot_sync(0xffffffffu, first_np < 8);
+      const uint32_t end_lane = np ? __ffs(np) - 1u : 32u;
+      T part = T(0);
+      const uint32_t upto = lane < end_lane ? 8u : (lane == end_lane ? first_np : 0u);
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j)
+        if (j < upto) part = add_rn(part, t[j]);
+      part = group_reduce_down(part, 32);
+      racc = add_rn(racc, __shfl_sync(0xffffffffu, part, 0));
+      if (np) {
+        end_tile = base + 8u * end_lane + __shfl_sync(0xffffffffu, first_np, end_lane);
+        break;
+      }
+      base += 256u;
+    }
+    if (lane == src) acc = add_rn(add_rn(acc, racc), cw.head[end_tile]);
+  }
+  if (chain) coo_put<T, ACCUM>(y, n_rows, row, acc);
 }
 
 // ---------------------------------------------------------------------------

@@ -166,18 +166,48 @@ __device__ __forceinline__ void stage_lowp(const lowp_args<VT, D16> &A, uint32_t
     dst[swz(e - base8)] = mul_rn(lowp_to_float<VT>(ld_stream_u16(A.vals + e, pol)), ld_x(A.x + lowp_col(A, e, pol)));
 }
 
+// Rows with more elements than this are summed by a warp (lane-strided, then a
+// shuffle tree) instead of by their own thread, so a row of 50,000 elements
+// costs its CTA ~1,600 steps per lane, not 50,000 in one thread.
+constexpr uint32_t kLowpAssist = 128;
+
 template <int VT, bool D16, bool VEC>
 __global__ void __launch_bounds__(kBlock, 6) lowp_kernel(const lowp_args<VT, D16> A) {
   __shared__ uint32_t s_rp[kBlock + 1];
+  __shared__ uint32_t s_assist[kBlock];
+  __shared__ uint32_t s_wc[kBlock / 32 + 1];
+  __shared__ float s_acc[kBlock];
   __shared__ __align__(16) float prod[kLowpChunk + 64];
   const uint64_t pol = policy_evict_first();
   const uint32_t r0 = blockIdx.x * kBlock;
   const uint32_t nr = min((uint32_t)kBlock, A.n_rows - r0);
-  const uint32_t t = threadIdx.x;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = t; i <= nr; i += kBlock) s_rp[i] = A.row_ptr[r0 + i];
+  s_acc[t] = 0.f;
   __syncthreads();
   const bool has = t < nr;
   const uint32_t rs = has ? s_rp[t] : 0u, re = has ? s_rp[t + 1] : 0u;
+  const bool assist = has && re - rs > kLowpAssist;
+  uint32_t nassist = 0;
+  if (__syncthreads_or(assist)) {
+    // ordered list of the block's long rows
+    const uint32_t ballot = __ballot_sync(0xffffffffu, assist);
+    if (lane == 0) s_wc[warp] = __popc(ballot);
+    __syncthreads();
+    if (t == 0) {
+      uint32_t sum = 0;
+      for (uint32_t w = 0; w < kBlock / 32; ++w) {
+        const uint32_t c = s_wc[w];
+        s_wc[w] = sum;
+        sum += c;
+      }
+      s_wc[kBlock / 32] = sum;
+    }
+    __syncthreads();
+    if (assist) s_assist[s_wc[warp] + __popc(ballot & ((1u << lane) - 1u))] = t;
+    __syncthreads();
+    nassist = s_wc[kBlock / 32];
+  }
   const uint32_t a = s_rp[0], b = s_rp[nr];
   float acc = 0.f;
   for (uint32_t c0 = a; c0 < b;) {
@@ -185,14 +215,25 @@ __global__ void __launch_bounds__(kBlock, 6) lowp_kernel(const lowp_args<VT, D16
     const uint32_t c1 = min(b, base8 + kLowpChunk);
     stage_lowp<VT, D16, VEC>(A, c0, c1, prod, pol);
     __syncthreads();
-    if (has) {
+    if (has && !assist) {
       const uint32_t lo = max(rs, c0), hi = min(re, c1);
       if (lo < hi) acc = seq_sum<float, true>(acc, prod, lo - base8, hi - base8);
+    }
+    for (uint32_t q = warp; q < nassist; q += kBlock / 32) {
+      const uint32_t j = s_assist[q];
+      const uint32_t js = s_rp[j], je = s_rp[j + 1];
+      const uint32_t lo = max(js, c0), hi = min(je, c1);
+      if (lo < hi) {
+        // lane l takes the row's elements js + l + 32 k, whichever chunk they fall in
+        float part = strided_sum(prod, lo - base8, hi - base8, (lane - (lo - js)) & 31u, 32u);
+        part = group_reduce_down(part, 32);
+        if (lane == 0) s_acc[j] = add_rn(s_acc[j], part);
+      }
     }
     __syncthreads();
     c0 = c1;
   }
-  if (has) A.y[r0 + t] = acc * A.scale[r0 + t];
+  if (has) A.y[r0 + t] = (assist ? s_acc[t] : acc) * A.scale[r0 + t];
 }
 
 // ---------------------------------------------------------------------------

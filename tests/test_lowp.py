@@ -94,10 +94,12 @@ def _check(oracle_lib, m, vt, y, x):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["stencil_32", "banded_100k", "power_law_100k"])
+@pytest.mark.parametrize("name", ["stencil_32", "banded_100k", "power_law_100k", "long_rows"])
 @pytest.mark.parametrize("vt", [BF16, F16])
 @pytest.mark.parametrize("index16", [False, True])
 def test_lowp_handle_accuracy(oracle_lib, name, vt, index16):
+    """Handles; matrices with rows longer than 1,024 elements (power_law_100k,
+    long_rows) run the row-block kernel, whose warps share the long rows."""
     import torch
     from matrix_format_performance_b200.device import DeviceMatrix
     m = case(name)
