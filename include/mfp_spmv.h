@@ -232,8 +232,11 @@ int mfp_dev_scratch_release(void);
 typedef enum mfp_csr_algo { MFP_CSR_SCALAR = 0, MFP_CSR_VECTOR = 1, MFP_CSR_ADAPTIVE = 2 } mfp_csr_algo;
 typedef struct mfp_csr_config {
   uint32_t long_row_threshold; /* 0 = default for the algo; UINT32_MAX = never split */
-  uint32_t vector_lanes;       /* CSR vector lanes per row: 2..32 (power of two); 0 = auto
-                                  (2 below a mean row length of 12, else 4) */
+  uint32_t vector_lanes;       /* CSR vector lanes per row: 2..32 (power of two); 0 = auto:
+                                  below a mean row length of 64 the warp-tile kernel (each
+                                  warp's lanes take 8 consecutive elements of 256 and combine
+                                  rows with a segmented shuffle scan; a fix-up launch adds the
+                                  rows that cross tiles), else 4 lanes per row */
   uint32_t bin_nnz;            /* CSR-Adaptive elements per row bin; 0 = default */
   uint32_t piece_nnz;          /* elements per long-row piece; 0 = default (4096) */
   uint32_t assist_threshold;   /* scalar/vector: rows longer than this (and not long) are
@@ -241,7 +244,9 @@ typedef struct mfp_csr_config {
                                   UINT32_MAX = never (keeps the reference summation order) */
   uint32_t kernel;             /* 0 = auto, 1 = row-block kernel (rows per CTA, long rows in
                                   pieces), 2 = streaming kernel (fixed element chunks per
-                                  persistent CTA, TMA bulk prefetch) */
+                                  persistent CTA, TMA bulk prefetch), 4 = warp-tile kernel
+                                  (256 consecutive elements per warp, rows from row_ptr,
+                                  segmented shuffle scan + a fix-up launch) */
 } mfp_csr_config;
 typedef struct mfp_csr_plan mfp_csr_plan;
 int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *host_row_ptr,
@@ -582,7 +587,11 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out);
 /* y = A*x with device x and y (value type of the matrix), enqueued on stream. */
 int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream);
 /* y = A*x with HOST x and y: copies x in, runs the kernel, copies y out, and
- * waits for the copy.  Page-locked host buffers give full PCIe bandwidth. */
+ * waits for the copy.  Page-locked host buffers give full PCIe bandwidth.
+ * When host_y is page-locked and device-addressable and the format's kernel
+ * stores each row of y once in row order (CSR scalar / adaptive, CSR vector
+ * with lanes per row, ELL, SCOO, the reduced-precision layouts), the kernel
+ * stores y straight into host_y, so the copy-out overlaps the kernel. */
 int mfp_matrix_spmv_host(mfp_matrix *m, const void *host_x, void *host_y, void *stream);
 
 /* ------------------------------------------------------------------------- */

@@ -172,6 +172,14 @@ struct mfp_csr_plan {
   uint32_t *counters = nullptr;
   uint32_t *row_blocks = nullptr;
   uint32_t *order = nullptr;  // work items heaviest first (n_main + n_pieces)
+  // warp-tile kernel (CSR vector on short rows): the row of the element before
+  // each 256-element tile, and the COO-style workspace of the fix-up pass
+  uint4 *blk = nullptr;  // per row block: element range and flags (see csr_args::blk)
+  bool fast = false;     // row blocks without long rows start their loads before the row_ptr barrier
+  bool tile = false;
+  uint32_t *tile_prev = nullptr;
+  void *tile_ws = nullptr;
+  size_t tile_ws_bytes = 0;
   size_t device_bytes = 0;
 };
 
@@ -181,6 +189,15 @@ struct mfp_csr_plan {
 #endif
 
 namespace {
+// COO workspace: a 16-byte header (the first and last row holding elements;
+// its error word stays 0: the two-pass COO has no waits) and, per 256-element
+// warp tile, the head and tail partial sums (8 bytes each, FP64-sized), the
+// flags and the tail row.  Every call rewrites what it reads: no
+// initialisation.
+size_t coo_ws_bytes(uint32_t nnz) {
+  const uint64_t wt = (nnz + (uint64_t)d::kWarpTile - 1) / d::kWarpTile;
+  return sizeof(d::coo_ws_header) + wt * 24u;
+}
 constexpr uint32_t kDefaultLong = 4096;
 constexpr uint32_t kDefaultAssist = 64;
 constexpr uint32_t kDefaultPiece = 4096;
@@ -318,6 +335,11 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
   }
   if (algo == MFP_CSR_VECTOR) {
     uint32_t L = cfg.vector_lanes;
+    // auto below a mean row length of 64: the warp-tile kernel, where lanes
+    // share rows through the segmented scan.  Measured on B200 against 2 and 4
+    // lanes per row: power-law 4M 0.187 ms (2 lanes 0.240), 27-point stencil
+    // 0.153 ms (0.178), banded 8M 0.599 ms (0.669), FP32.
+    plan->tile = L == 0 && cfg.kernel == 0 && rows && (double)nnz / rows < 64.0;
     if (L == 0) {
       // Measured on B200 over 2,200 seeded matrices (uniform, Zipf, banded,
       // block-diagonal, stencil, dense-row families) and the 4M-row power-law
@@ -334,6 +356,8 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
     }
     cfg.vector_lanes = L;
   }
+  if (cfg.kernel == 4) plan->tile = true;  // the warp-tile kernel on request, any algorithm
+  if (nnz == 0) plan->tile = false;
   plan->assist_thr = cfg.assist_threshold ? cfg.assist_threshold : kDefaultAssist;
   plan->cfg = cfg;
 
@@ -421,6 +445,47 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
     mfp_csr_plan_destroy(plan);
     return st;
   }
+  // row blocks that start their loads before the row_ptr barrier: measured
+  // faster for lanes per row and for long rows (mean length 16 and up)
+  plan->fast = algo != MFP_CSR_ADAPTIVE && (algo == MFP_CSR_VECTOR || (rows && (double)nnz / rows >= 16.0));
+  if (plan->fast) {
+    // per row block: its element range and whether it holds a long or an
+    // assisted row
+    std::vector<uint4> br(plan->n_main);
+    for (uint32_t b = 0; b < plan->n_main; ++b) {
+      const uint32_t r0 = b * d::kBlock;
+      const uint32_t r1 = std::min(rows, r0 + d::kBlock);
+      uint32_t flags = 0;
+      for (uint32_t r = r0; r < r1; ++r) {
+        const uint32_t len = rp[r + 1] - rp[r];
+        if (len > cfg.long_row_threshold) flags |= 1u;
+        else if (len > plan->assist_thr) flags |= 2u;
+      }
+      br[b] = make_uint4(rp[r0], rp[r1], flags, 0u);
+    }
+    if ((st = upload(&plan->blk, br.data(), br.size(), &plan->device_bytes))) {
+      mfp_csr_plan_destroy(plan);
+      return st;
+    }
+  }
+  if (plan->tile) {
+    // the row holding element 256 w - 1, for every warp tile w > 0
+    const uint32_t n_wt = ceil_div(nnz, d::kWarpTile);
+    std::vector<uint32_t> prev(n_wt);
+    prev[0] = d::kNoRow;
+    for (uint32_t w = 1; w < n_wt; ++w) {
+      const uint32_t e = w * d::kWarpTile - 1u;
+      prev[w] = (uint32_t)(std::upper_bound(rp, rp + rows + 1, e) - rp) - 1u;
+    }
+    plan->tile_ws_bytes = coo_ws_bytes(nnz);
+    unsigned char *ws = nullptr;
+    if ((st = upload(&plan->tile_prev, prev.data(), prev.size(), &plan->device_bytes)) ||
+        (st = dmalloc(&ws, plan->tile_ws_bytes, &plan->device_bytes))) {
+      mfp_csr_plan_destroy(plan);
+      return st;
+    }
+    plan->tile_ws = ws;
+  }
   if (nlong) {
     const cudaError_t e = cudaMemset(plan->counters, 0, nlong * sizeof(uint32_t));
     if (e != cudaSuccess) {
@@ -440,6 +505,9 @@ extern "C" int mfp_csr_plan_destroy(mfp_csr_plan *plan) {
   cudaFree(plan->row_blocks);
   cudaFree(plan->order);
   cudaFree(plan->error);
+  cudaFree(plan->tile_prev);
+  cudaFree(plan->tile_ws);
+  cudaFree(plan->blk);
   free_stream_plan(plan->sp[0]);
   free_stream_plan(plan->sp[1]);
   delete plan;
@@ -475,6 +543,10 @@ void launch_stream(int algo, uint32_t grid, cudaStream_t s, const d::stream_args
 }
 
 template <typename T>
+int csr_tile_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, const uint32_t *rp, const T *x,
+                  T *y, cudaStream_t s);
+
+template <typename T>
 int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, const uint32_t *rp, const T *x,
              T *y, void *stream) {
   if (!plan) return fail(MFP_ERROR_INVALID_VALUE, "plan is NULL");
@@ -497,6 +569,7 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
   A.partials = plan->partials;
   A.counters = plan->counters;
   A.order = MFP_CSR_ORDER ? plan->order : nullptr;
+  A.blk = plan->blk;
   const bool vec = aligned16(data) && aligned16(cols);
   cudaStream_t s = as_stream(stream);
   if (plan->nnz == 0) return fill<T>(plan->rows, y, T(0), stream);
@@ -530,17 +603,23 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
       launch_stream<T, 0>(plan->algo, sp.grid, s, S);
     return check_launch("csr_stream_kernel launch");
   }
+  if (plan->tile && !exact_order) return csr_tile_spmv<T>(plan, data, cols, rp, x, y, s);
   const uint32_t grid = plan->n_main + plan->n_pieces;
   if (grid == 0) return ok();
-#define MFP_CSR_LAUNCH(ALGO)                                                         \
+#define MFP_CSR_LAUNCH(ALGO, FAST)                                                   \
   if (vec)                                                                           \
-    d::csr_kernel<T, ALGO, true><<<grid, d::kBlock, 0, s>>>(A);                      \
+    d::csr_kernel<T, ALGO, true, FAST><<<grid, d::kBlock, 0, s>>>(A);                \
   else                                                                               \
-    d::csr_kernel<T, ALGO, false><<<grid, d::kBlock, 0, s>>>(A);
+    d::csr_kernel<T, ALGO, false, FAST><<<grid, d::kBlock, 0, s>>>(A);
+  const bool fast = plan->fast && plan->blk;
   switch (plan->algo) {
-    case 0: MFP_CSR_LAUNCH(0) break;
-    case 1: MFP_CSR_LAUNCH(1) break;
-    default: MFP_CSR_LAUNCH(2) break;
+    case 0:
+      if (fast) { MFP_CSR_LAUNCH(0, true) } else { MFP_CSR_LAUNCH(0, false) }
+      break;
+    case 1:
+      if (fast) { MFP_CSR_LAUNCH(1, true) } else { MFP_CSR_LAUNCH(1, false) }
+      break;
+    default: MFP_CSR_LAUNCH(2, false) break;
   }
 #undef MFP_CSR_LAUNCH
   return check_launch("csr_kernel launch");
@@ -594,15 +673,6 @@ cudaError_t launch_after(void (*k)(KArgs...), uint32_t grid, cudaStream_t s, Arg
   return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 
-// COO workspace: a 16-byte header (the first and last row holding elements;
-// its error word stays 0: the two-pass COO has no waits) and, per 256-element
-// warp tile, the head and tail partial sums (8 bytes each, FP64-sized), the
-// flags and the tail row.  Every call rewrites what it reads: no
-// initialisation.
-size_t coo_ws_bytes(uint32_t nnz) {
-  const uint64_t wt = (nnz + (uint64_t)d::kWarpTile - 1) / d::kWarpTile;
-  return sizeof(d::coo_ws_header) + wt * 24u;
-}
 
 template <typename T, bool ACCUM = false>
 int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
@@ -646,6 +716,32 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
     e = launch_after(d::coo_fixup_kernel<T, ACCUM>, fgrid, s, n_wt, rows, cw, (const d::coo_ws_header *)hdr, y);
     if (e != cudaSuccess) return cuda_fail(e, "coo_fixup_kernel launch");
   }
+  return ok();
+}
+
+// The warp-tile CSR (CSR vector on short rows): warp pass + the COO fix-up.
+template <typename T>
+int csr_tile_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, const uint32_t *rp, const T *x,
+                  T *y, cudaStream_t s) {
+  const uint32_t nnz = plan->nnz, rows = plan->rows;
+  const uint32_t n_wt = ceil_div(nnz, d::kWarpTile);
+  auto *hdr = static_cast<d::coo_ws_header *>(plan->tile_ws);
+  unsigned char *base = static_cast<unsigned char *>(plan->tile_ws) + sizeof(d::coo_ws_header);
+  d::coo_carry<T> cw;
+  cw.head = reinterpret_cast<T *>(base);
+  cw.tail = reinterpret_cast<T *>(base + (size_t)n_wt * 8u);
+  cw.flags = reinterpret_cast<uint32_t *>(base + (size_t)n_wt * 16u);
+  cw.tail_row = cw.flags + n_wt;
+  const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
+  if (aligned16(data) && aligned16(cols))
+    d::csr_tile_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rp, plan->tile_prev, x, y, cw, hdr);
+  else
+    d::csr_tile_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rp, plan->tile_prev, x, y, cw, hdr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "csr_tile_kernel launch");
+  const uint32_t fgrid = std::max(ceil_div(n_wt, d::kBlock), std::min(ceil_div(rows, d::kBlock * 8u), 148u * 4u));
+  e = launch_after(d::coo_fixup_kernel<T, false>, fgrid, s, n_wt, rows, cw, (const d::coo_ws_header *)hdr, y);
+  if (e != cudaSuccess) return cuda_fail(e, "coo_fixup_kernel launch");
   return ok();
 }
 
@@ -770,13 +866,18 @@ int lowp_spmv(int vt, uint32_t rows, uint32_t nnz, const uint32_t *rp, const uin
   return check_launch("lowp_kernel launch");
 }
 
+// Runs of 8 consecutive x entries read with 16-byte loads where a lane's rows
+// share a column offset (1), or always 8 gathers (0).
+#ifndef MFP_LOWP_XRUN
+#define MFP_LOWP_XRUN 1
+#endif
 // The 16-bit ELL kernel's VEC path (8 consecutive rows per thread, 16-byte
 // loads) when the layout allows it (1), or always the lane-interleaved path (0).
 #ifndef MFP_LOWP_ELL_VEC
 #define MFP_LOWP_ELL_VEC 1
 #endif
-int lowp_ell_spmv(int vt, uint32_t rows, uint32_t width, const uint16_t *q, const float *scale, const uint32_t *cols,
-                  const uint16_t *off, const float *x, float *y, void *stream) {
+int lowp_ell_spmv(int vt, uint32_t rows, uint32_t cols_n, uint32_t width, const uint16_t *q, const float *scale,
+                  const uint32_t *cols, const uint16_t *off, const float *x, float *y, void *stream) {
   if (vt != MFP_BF16 && vt != MFP_F16) return fail(MFP_ERROR_INVALID_VALUE, "value type must be BF16 or F16");
   if (rows == 0) return ok();
   if (!scale || !y || (width && (!q || !x || (!cols && !off)))) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
@@ -786,8 +887,10 @@ int lowp_ell_spmv(int vt, uint32_t rows, uint32_t width, const uint16_t *q, cons
   const uint32_t grid = ceil_div(ceil_div(rows, 8), d::kBlock);
 #define MFP_LELL(VT, D16)                                                                         \
   {                                                                                               \
-    d::lowp_ell_args<VT, D16> A{rows, width, q, scale, cols, off, x, y};                          \
-    if (vec)                                                                                      \
+    d::lowp_ell_args<VT, D16> A{rows, width, cols_n, q, scale, cols, off, x, y};                  \
+    if (MFP_LOWP_XRUN && vec && D16 && aligned16(x))                                              \
+      d::lowp_ell_kernel<VT, D16, true, true><<<grid, d::kBlock, 0, s>>>(A);                      \
+    else if (vec)                                                                                 \
       d::lowp_ell_kernel<VT, D16, true><<<grid, d::kBlock, 0, s>>>(A);                            \
     else                                                                                          \
       d::lowp_ell_kernel<VT, D16, false><<<grid, d::kBlock, 0, s>>>(A);                           \
@@ -900,9 +1003,9 @@ int mfp_lowp_spmv(int vt, uint32_t rows, uint32_t, uint32_t nnz, const uint32_t 
                   const float *x, float *y, void *s) {
   return lowp_spmv(vt, rows, nnz, rp, q, scale, cols, delta, base, x, y, s);
 }
-int mfp_lowp_ell_spmv(int vt, uint32_t rows, uint32_t, uint32_t width, const uint16_t *q, const float *scale,
+int mfp_lowp_ell_spmv(int vt, uint32_t rows, uint32_t ncols, uint32_t width, const uint16_t *q, const float *scale,
                       const uint32_t *cols, const uint16_t *off, const float *x, float *y, void *s) {
-  return lowp_ell_spmv(vt, rows, width, q, scale, cols, off, x, y, s);
+  return lowp_ell_spmv(vt, rows, ncols, width, q, scale, cols, off, x, y, s);
 }
 }  // extern "C"
 template <int MODE, int XPATH>
@@ -1575,6 +1678,8 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
     out->kernel_launches = m->nnz ? 2u : (m->rows ? 1u : 0u);
   else if (m->format == MFP_FORMAT_HYBRID)
     out->kernel_launches = 1u + (m->coo_nnz ? (m->coo_nnz > d::kWarpTile ? 2u : 1u) : 0u);
+  else if (m->plan && m->plan->tile)  // CSR vector on short rows: warp pass + fix-up
+    out->kernel_launches = 2u;
   else
     out->kernel_launches = 1u;
   return ok();
@@ -1622,7 +1727,7 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                                    (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
                                    m->ws_bytes, stream);
     case MFP_FORMAT_ELL_LOWP:
-      return lowp_ell_spmv(m->lowp_vt, m->rows, m->width, (const uint16_t *)m->vals, m->scale,
+      return lowp_ell_spmv(m->lowp_vt, m->rows, m->cols, m->width, (const uint16_t *)m->vals, m->scale,
                            m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);
     case MFP_FORMAT_CSR_LOWP:
       return lowp_spmv(m->lowp_vt, m->rows, (uint32_t)m->nnz, m->rows_a, (const uint16_t *)m->vals, m->scale,
@@ -1633,15 +1738,45 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
   }
 }
 
+// Formats whose kernels write each row of y once, a warp's stores covering
+// consecutive rows: their y can go straight into a page-locked host buffer.
+static bool writes_y_in_row_order(const mfp_matrix *m) {
+  if (m->plan && (m->plan->cfg.kernel == 2 || m->plan->cfg.kernel == 3)) return false;  // streaming CSR
+  switch (m->format) {
+    case MFP_FORMAT_CSR_SCALAR:
+    case MFP_FORMAT_CSR_ADAPTIVE:
+    case MFP_FORMAT_ELL:
+    case MFP_FORMAT_SCOO:
+    case MFP_FORMAT_CSR_LOWP:
+    case MFP_FORMAT_ELL_LOWP:
+      return !(m->plan && m->plan->tile) && !m->rows_unsorted;
+    case MFP_FORMAT_CSR_VECTOR:
+      return !(m->plan && m->plan->tile);
+    default:  // COO and the warp-tile kernels write rows as their tiles finish; the hybrid adds into y
+      return false;
+  }
+}
+
 int mfp_matrix_spmv_host(mfp_matrix *m, const void *hx, void *hy, void *stream) {
   if (!m || !hy || (!hx && m->cols)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   const size_t vs = value_size(m->value_type);
   cudaStream_t s = as_stream(stream);
+  // a page-locked y (cudaHostAlloc / cudaHostRegister) that the device can
+  // address takes the kernel's stores directly, so the copy-out overlaps the
+  // kernel instead of following it
+  void *y_mapped = nullptr;
+  if (m->rows && writes_y_in_row_order(m)) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, hy) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer)
+      y_mapped = a.devicePointer;
+    else
+      cudaGetLastError();
+  }
   if (m->cols)
     CUDA_TRY(cudaMemcpyAsync(m->dx, hx, (size_t)m->cols * vs, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync x");
-  int st = mfp_matrix_spmv(m, m->dx, m->dy, stream);
+  int st = mfp_matrix_spmv(m, m->dx, y_mapped ? y_mapped : m->dy, stream);
   if (st) return st;
-  if (m->rows)
+  if (m->rows && !y_mapped)
     CUDA_TRY(cudaMemcpyAsync(hy, m->dy, (size_t)m->rows * vs, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync y");
   CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   return ok();

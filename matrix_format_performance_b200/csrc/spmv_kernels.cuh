@@ -669,6 +669,9 @@ struct csr_args {
   // work item of each block index (w < n_main: row block / bin w, else piece
   // w - n_main), heaviest first; NULL = blocks in index order
   const uint32_t *__restrict__ order;
+  // per row block (plan, row-block algorithms): element range [x, y);
+  // z bit 0 = has a long row, bit 1 = has an assisted row
+  const uint4 *__restrict__ blk;
 };
 
 template <typename T>
@@ -720,12 +723,120 @@ __device__ __forceinline__ uint32_t compact_ordered(bool flag, uint32_t value, u
 //   vector: row j is reduced by lane group j % (256/L), lane l taking the
 //           elements rs + l + k*L, then a shuffle tree over the group;
 // and in both, rows above the assist threshold are reduced by a warp.
+//
+// The reduction of one staged chunk [c0, c1) (local base `base`) for the rows
+// [run_lo, run_hi) of the block.
+template <typename T, int MODE>
+__device__ __forceinline__ void rowblock_chunk(const csr_args<T> &A, csr_smem<T> &sm, uint32_t run_lo,
+                                               uint32_t run_hi, uint32_t c0, uint32_t c1, uint32_t base, bool own,
+                                               uint32_t rs, uint32_t re, uint32_t nassist, T &acc) {
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  if (MODE == 0) {
+    if (own && t >= run_lo && t < run_hi) {
+      const uint32_t lo = max(rs, c0), hi = min(re, c1);
+      if (lo < hi) acc = seq_sum<T, false>(acc, sm.m.prod, lo - base, hi - base);
+    }
+  } else {
+    const uint32_t L = A.lanes;
+    // rows of the run that intersect [c0, c1): [jlo, jhi), by binary search
+    uint32_t jlo, jhi;
+    {
+      uint32_t lo_ = run_lo, hi_ = run_hi;  // first j with rp[j + 1] > c0
+      while (lo_ < hi_) {
+        const uint32_t mid = (lo_ + hi_) >> 1;
+        if (sm.m.rp[mid + 1] > c0) hi_ = mid; else lo_ = mid + 1;
+      }
+      jlo = lo_;
+      hi_ = run_hi;  // first j with rp[j] >= c1
+      while (lo_ < hi_) {
+        const uint32_t mid = (lo_ + hi_) >> 1;
+        if (sm.m.rp[mid] >= c1) hi_ = mid; else lo_ = mid + 1;
+      }
+      jhi = lo_;
+    }
+    const uint32_t G = kBlock / L, g = t / L, gl = t % L;
+    const uint32_t rounds = (jhi - jlo + G - 1u) / G;  // uniform over the CTA
+    for (uint32_t it = 0; it < rounds; ++it) {
+      const uint32_t j = jlo + g + it * G;
+      T part = T(0);
+      bool valid = false;
+      if (j < jhi) {
+        const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
+        const uint32_t len = je - js;
+        if (len <= A.assist_thr) {
+          const uint32_t s = max(js, c0), e = min(je, c1);
+          if (s < e) {
+            valid = true;
+            part = strided_sum(sm.m.prod, s - base, e - base, (gl - (s - js)) & (L - 1u), L);
+          }
+        }
+      }
+      part = group_reduce_down(part, (int)L);
+      if (valid && gl == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
+    }
+  }
+  // rows above the assist threshold: one warp per row segment
+  for (uint32_t q = warp; q < nassist; q += kBlock / 32) {
+    const uint32_t j = sm.m.assists[q];
+    const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
+    const uint32_t s = max(js, c0), e = min(je, c1);
+    if (s < e) {
+      T part = strided_sum(sm.m.prod, s - base, e - base, (lane - (s - js)) & 31u, 32u);
+      part = group_reduce_down(part, 32);
+      if (lane == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
+    }
+  }
+}
+
+// Blocks without long rows (their element range [a, b) from the plan): the
+// first chunk's loads and x gathers are issued together with the row_ptr
+// window's, before the first barrier.  A separate instantiation (FAST), since
+// the extra state costs registers: measured faster on long rows (banded 8M,
+// mean 32: CSR scalar 0.424 -> 0.404 ms) and for lanes per row (0.669 ->
+// 0.596 ms), slower on the power-law matrix (mean 7.5: 0.191 -> 0.199 ms).
 template <typename T, int MODE, bool VEC>
+__device__ __forceinline__ void csr_rowblock_fast(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol, uint32_t r0,
+                                                  uint32_t nr, uint4 br) {
+  const uint32_t t = threadIdx.x;
+  const uint32_t a = br.x, b = br.y;
+  for (uint32_t i = t; i <= nr; i += kBlock) sm.m.rp[i] = A.row_ptr[r0 + i];
+  sm.m.acc[t] = T(0);
+  uint32_t c0 = a, base = a & ~3u;
+  uint32_t c1 = min(b, base + (uint32_t)kChunk);
+  if (c0 < c1) stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, c0, c1, sm.m.prod, nullptr, pol);
+  __syncthreads();
+  const bool has = t < nr;
+  const uint32_t rs = has ? sm.m.rp[t] : 0u, re = has ? sm.m.rp[t + 1] : 0u;
+  const bool is_assist = has && (re - rs > A.assist_thr);
+  uint32_t nassist = 0;
+  if (br.z & 2u) nassist = compact_ordered<T>(is_assist, t, sm.m.assists, sm, &sm.m.nassist);
+  T acc = T(0);
+  for (;;) {
+    rowblock_chunk<T, MODE>(A, sm, 0u, nr, c0, c1, base, has && !is_assist, rs, re, nassist, acc);
+    __syncthreads();
+    if (c1 >= b) break;
+    c0 = c1;
+    base = c0 & ~3u;
+    c1 = min(b, base + (uint32_t)kChunk);
+    stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, c0, c1, sm.m.prod, nullptr, pol);
+    __syncthreads();
+  }
+  if (has) A.y[r0 + t] = (MODE == 0 && !is_assist) ? acc : sm.m.acc[t];
+}
+
+template <typename T, int MODE, bool VEC, bool FAST>
 __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol,
                                                   uint32_t blk) {
   const uint32_t r0 = blk * kBlock;
   const uint32_t nr = min((uint32_t)kBlock, A.n_rows - r0);
-  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t t = threadIdx.x;
+  if (FAST) {
+    const uint4 br = A.blk[blk];
+    if (!(br.z & 1u)) {
+      csr_rowblock_fast<T, MODE, VEC>(A, sm, pol, r0, nr, br);
+      return;
+    }
+  }
   for (uint32_t i = t; i <= nr; i += kBlock) sm.m.rp[i] = A.row_ptr[r0 + i];
   if (t < kBlock) sm.m.acc[t] = T(0);
   __syncthreads();
@@ -738,7 +849,6 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
     nlong = compact_ordered<T>(is_long, t, sm.m.longs, sm, &sm.m.nlong);
     nassist = compact_ordered<T>(is_assist, t, sm.m.assists, sm, &sm.m.nassist);
   }
-  const uint32_t L = (MODE == 1) ? A.lanes : 1u;
   T acc = T(0);  // scalar: running sum of this thread's row
   uint32_t run_lo = 0;
   for (uint32_t k = 0; k <= nlong; ++k) {
@@ -750,60 +860,8 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
         const uint32_t c1 = min(b, base + (uint32_t)kChunk);
         stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, c0, c1, sm.m.prod, nullptr, pol);
         __syncthreads();
-        if (MODE == 0) {
-          if (has && !is_long && !is_assist && t >= run_lo && t < run_hi) {
-            const uint32_t lo = max(rs, c0), hi = min(re, c1);
-            if (lo < hi) acc = seq_sum<T, false>(acc, sm.m.prod, lo - base, hi - base);
-          }
-        } else {
-          // rows of the run that intersect [c0, c1): [jlo, jhi), by binary search
-          uint32_t jlo, jhi;
-          {
-            uint32_t lo_ = run_lo, hi_ = run_hi;  // first j with rp[j + 1] > c0
-            while (lo_ < hi_) {
-              const uint32_t mid = (lo_ + hi_) >> 1;
-              if (sm.m.rp[mid + 1] > c0) hi_ = mid; else lo_ = mid + 1;
-            }
-            jlo = lo_;
-            hi_ = run_hi;  // first j with rp[j] >= c1
-            while (lo_ < hi_) {
-              const uint32_t mid = (lo_ + hi_) >> 1;
-              if (sm.m.rp[mid] >= c1) hi_ = mid; else lo_ = mid + 1;
-            }
-            jhi = lo_;
-          }
-          const uint32_t G = kBlock / L, g = t / L, gl = t % L;
-          const uint32_t rounds = (jhi - jlo + G - 1u) / G;  // uniform over the CTA
-          for (uint32_t it = 0; it < rounds; ++it) {
-            const uint32_t j = jlo + g + it * G;
-            T part = T(0);
-            bool valid = false;
-            if (j < jhi) {
-              const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
-              const uint32_t len = je - js;
-              if (len <= A.assist_thr) {
-                const uint32_t s = max(js, c0), e = min(je, c1);
-                if (s < e) {
-                  valid = true;
-                  part = strided_sum(sm.m.prod, s - base, e - base, (gl - (s - js)) & (L - 1u), L);
-                }
-              }
-            }
-            part = group_reduce_down(part, (int)L);
-            if (valid && gl == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
-          }
-        }
-        // rows above the assist threshold: one warp per row segment
-        for (uint32_t q = warp; q < nassist; q += kBlock / 32) {
-          const uint32_t j = sm.m.assists[q];
-          const uint32_t js = sm.m.rp[j], je = sm.m.rp[j + 1];
-          const uint32_t s = max(js, c0), e = min(je, c1);
-          if (s < e) {
-            T part = strided_sum(sm.m.prod, s - base, e - base, (lane - (s - js)) & 31u, 32u);
-            part = group_reduce_down(part, 32);
-            if (lane == 0) sm.m.acc[j] = add_rn(sm.m.acc[j], part);
-          }
-        }
+        rowblock_chunk<T, MODE>(A, sm, run_lo, run_hi, c0, c1, base, has && !is_long && !is_assist, rs, re,
+                                nassist, acc);
         __syncthreads();
         c0 = c1;
       }
@@ -863,7 +921,7 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
   }
 }
 
-template <typename T, int ALGO, bool VEC>
+template <typename T, int ALGO, bool VEC, bool FAST = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? (ALGO != 1 ? MFP_CSR_MINBLOCKS : MFP_CSR_MINBLOCKS_VEC) : (ALGO == 0 ? MFP_CSR_MINBLOCKS64 : MFP_CSR_MINBLOCKS64_OTHER)) csr_kernel(const csr_args<T> A) {
   __shared__ csr_smem<T> sm;
   const uint64_t pol = policy_evict_first();
@@ -886,7 +944,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? (ALGO != 1 ? MFP_CSR_
   if (ALGO == 2)
     csr_adaptive_main<T, VEC>(A, sm, pol, b);
   else
-    csr_rowblock_main<T, ALGO, VEC>(A, sm, pol, b);
+    csr_rowblock_main<T, ALGO, VEC, FAST>(A, sm, pol, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -1089,6 +1147,109 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
   const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
   const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
   warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw, hdr);
+}
+
+// ---------------------------------------------------------------------------
+// CSR in warp tiles: the COO warp pass with each element's row taken from
+// row_ptr instead of a stored row id.  Warp w owns the 256 elements
+// [256 w, 256 w + 256); while their values, column ids and x gathers are in
+// flight, the warp reads the row starts that fall inside the tile
+// (row_ptr[prev + 1 ...], 32 per round; prev = the row of element 256 w - 1,
+// from the plan), counts them per element position in shared memory, and a
+// prefix count gives every element its row.  The reduction and the fix-up
+// pass are the COO ones.  Used for CSR vector on short rows: the lanes of a
+// warp share the rows' elements (8 each) and combine them with the segmented
+// shuffle scan, whatever the rows' lengths.
+// ---------------------------------------------------------------------------
+template <typename T, bool VEC>
+__device__ __forceinline__ uint32_t load_product_group(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                                       const T *__restrict__ x, uint32_t g, uint32_t c1,
+                                                       T (&p)[kEpt], uint64_t pol) {
+  if (g >= c1) return 0u;
+  const uint32_t cnt = min(kEpt, c1 - g);
+  if (VEC && cnt == kEpt) {  // g a multiple of 8: 16-byte aligned for 4-byte types
+    T v0[4], v1[4];
+    uint32_t k0[4], k1[4];
+    ld_stream4(vals + g, v0, pol);
+    ld_stream4(vals + g + 4, v1, pol);
+    ld_stream4(cols + g, k0, pol);
+    ld_stream4(cols + g + 4, k1, pol);
+    T x0[4], x1[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x0[k] = ld_x(x + k0[k]);
+      x1[k] = ld_x(x + k1[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      p[k] = mul_rn(v0[k], x0[k]);
+      p[4 + k] = mul_rn(v1[k], x1[k]);
+    }
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < kEpt; ++k)
+      if (k < cnt) p[k] = mul_rn(ld_stream1(vals + g + k, pol), ld_x(x + ld_stream1(cols + g + k, pol)));
+  }
+  return cnt;
+}
+
+constexpr uint32_t kTileCnt = kWarpTile + 4;  // per-warp start counts: positions 0..256, padded to 16 bytes
+
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
+    csr_tile_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                    const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ tile_prev,
+                    const T *__restrict__ x, T *__restrict__ y, coo_carry<T> cw, coo_ws_header *hdr) {
+  __shared__ __align__(16) uint32_t s_cnt[kBlock / 32][kTileCnt];
+  const uint64_t pol = policy_evict_first();
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t wt = blockIdx.x * (kBlock / 32) + warp;
+  if ((uint64_t)wt * kWarpTile >= nnz) return;  // whole warps only
+  const uint32_t c0 = wt * kWarpTile, c1 = min(nnz, c0 + kWarpTile);
+  T pr[kEpt];
+  const uint32_t g = c0 + lane * kEpt;
+  const uint32_t cnt = load_product_group<T, VEC>(vals, cols, x, g, c1, pr, pol);
+  uint32_t *sc = s_cnt[warp];
+  for (uint32_t i = lane; i < kTileCnt; i += 32u) sc[i] = 0u;
+  const uint32_t prv = __ldg(tile_prev + wt);  // row of element c0 - 1; kNoRow for the first tile
+  // row starts at positions [c0, lim]: lim = c1 locates the row after the
+  // tile, which the last tile does not need
+  const uint32_t lim = c1 < nnz ? c1 : c1 - 1u;
+  __syncwarp();
+  for (uint32_t j0 = prv + 1u;; j0 += 32u) {  // prv + 1 wraps to 0 for the first tile
+    const uint32_t j = j0 + lane;
+    const uint32_t b = j < n_rows ? __ldg(row_ptr + j) : 0xffffffffu;  // start of row j (>= c0)
+    if (b <= lim) atomicAdd(&sc[b - c0], 1u);
+    if (__any_sync(0xffffffffu, b > lim)) break;
+  }
+  __syncwarp();
+  // row of each element: prv + the row starts at or before it
+  uint32_t q[kEpt];
+  {
+    const uint4 a = *reinterpret_cast<const uint4 *>(sc + lane * kEpt);
+    const uint4 b = *reinterpret_cast<const uint4 *>(sc + lane * kEpt + 4);
+    q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = a.w;
+    q[4] = b.x; q[5] = b.y; q[6] = b.z; q[7] = b.w;
+  }
+  uint32_t tot = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kEpt; ++k) tot += q[k];
+  uint32_t inc = tot;  // inclusive scan of the lanes' counts
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  const uint32_t all = __shfl_sync(0xffffffffu, inc, 31);
+  uint32_t rw[kEpt];
+  uint32_t run = prv + (inc - tot);
+#pragma unroll
+  for (uint32_t k = 0; k < kEpt; ++k) {
+    run += q[k];
+    rw[k] = run;
+  }
+  const uint32_t nxt = c1 < nnz ? prv + all + sc[kWarpTile] : kNoRow;  // row of element c1
+  warp_tile_reduce<T, false>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw, hdr);
 }
 
 // Pass 2: the row starting in tile w that continues past it.  The tiles that

@@ -564,10 +564,15 @@ __global__ void __launch_bounds__(kLowpThreads, 3) lowp_tma_kernel(const lowp_ar
 // rows interleaved across its warp (row = warp base + 32 j + lane), so each
 // 2-byte load and each x gather is contiguous over the warp.  Slots in order
 // 0..width-1, FMA accumulation; y = acc * scale.
+// With 16-bit offsets, a lane whose 8 rows have the same offset in a slot
+// (stencil rows away from the grid's faces) reads their 8 consecutive x
+// entries with two or three 16-byte loads instead of 8 gathers: a warp's
+// x reads then cover 8 cache lines per instruction instead of 32 sectors,
+// which lifts the L1 limit of the gathers.  Other lanes gather.
 // ---------------------------------------------------------------------------
 template <int VT, bool D16>
 struct lowp_ell_args {
-  uint32_t n_rows, width;
+  uint32_t n_rows, width, n_cols;
   const uint16_t *__restrict__ q;
   const float *__restrict__ scale;
   const uint32_t *__restrict__ cols;  // !D16
@@ -576,8 +581,26 @@ struct lowp_ell_args {
   float *__restrict__ y;
 };
 
-template <int VT, bool D16, bool VEC>
-__global__ void __launch_bounds__(kBlock) lowp_ell_kernel(const lowp_ell_args<VT, D16> A) {
+// CTAs per SM the 16-bit ELL kernel is register-limited to: 8 (32 registers)
+// holds the 27-point 128^3 stencil's 1,024 CTAs in one wave on 148 SMs
+// (6, at 40 registers, left a second wave of 136 CTAs).
+#ifndef MFP_LOWP_ELL_MINBLOCKS
+#define MFP_LOWP_ELL_MINBLOCKS 8
+#endif
+
+// x[c .. c + 7] from the 16-byte-aligned words at c & ~3 (needs (c & ~3) + 12 <= n).
+__device__ __forceinline__ void ld_x8_run(const float *__restrict__ x, uint32_t c, float (&xv)[8]) {
+  const uint32_t a = c & ~3u, sh = c & 3u;
+  const float4 v0 = __ldg(reinterpret_cast<const float4 *>(x + a));
+  const float4 v1 = __ldg(reinterpret_cast<const float4 *>(x + a + 4));
+  const float4 v2 = sh ? __ldg(reinterpret_cast<const float4 *>(x + a + 8)) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float w[12] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w, v2.x, v2.y, v2.z, v2.w};
+#pragma unroll
+  for (int j = 0; j < 8; ++j) xv[j] = sh == 0 ? w[j] : sh == 1 ? w[j + 1] : sh == 2 ? w[j + 2] : w[j + 3];
+}
+
+template <int VT, bool D16, bool VEC, bool XRUN = false>
+__global__ void __launch_bounds__(kBlock, MFP_LOWP_ELL_MINBLOCKS) lowp_ell_kernel(const lowp_ell_args<VT, D16> A) {
   const uint64_t pol = policy_evict_first();
   const size_t stride = A.n_rows;
   if (VEC) {
@@ -591,6 +614,7 @@ __global__ void __launch_bounds__(kBlock) lowp_ell_kernel(const lowp_ell_args<VT
       const size_t o = (size_t)k * stride + r;
       uint32_t qv[4], c[8];
       ld_stream8_u16(A.q + o, qv, pol);
+      bool run = false;
       if (D16) {
         uint32_t dv[4];
         ld_stream8_u16(A.off + o, dv, pol);
@@ -598,6 +622,11 @@ __global__ void __launch_bounds__(kBlock) lowp_ell_kernel(const lowp_ell_args<VT
         for (int j = 0; j < 4; ++j) {
           c[2 * j] = r + 2u * j + (dv[j] & 0xffffu) - 32768u;
           c[2 * j + 1] = r + 2u * j + 1u + (dv[j] >> 16) - 32768u;
+        }
+        if (XRUN) {
+          // the 8 rows share one offset: their columns are c[0] .. c[0] + 7
+          const uint32_t d2 = (dv[0] & 0xffffu) | (dv[0] << 16);
+          run = dv[0] == d2 && dv[1] == d2 && dv[2] == d2 && dv[3] == d2 && (c[0] & ~3u) + 12u <= A.n_cols;
         }
       } else {
         uint32_t c0[4], c1[4];
@@ -610,8 +639,12 @@ __global__ void __launch_bounds__(kBlock) lowp_ell_kernel(const lowp_ell_args<VT
         }
       }
       float xv[8];
+      if (run) {
+        ld_x8_run(A.x, c[0], xv);
+      } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) xv[j] = ld_x(A.x + c[j]);
+        for (int j = 0; j < 8; ++j) xv[j] = ld_x(A.x + c[j]);
+      }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const float2 f = lowp_pair<VT>(qv[j]);

@@ -47,11 +47,15 @@ CONFIGS: list[tuple[str, dict] | None] = [
     ("ell", {}), None, None, None,
     # COO (one layout)
     ("coo", {}), None, None, None,
-    # SCOO: shared memory per block the slice size is derived from
-    ("scoo", {"shared_mem": 49152}), ("scoo", {"shared_mem": 24576}), ("scoo", {"shared_mem": 98304}), None,
-    # hybrid: ELL width at a row-length quantile, or the reference's percent rule
-    ("hybrid", {"quantile": 0.5}), ("hybrid", {"quantile": 2 / 3}), ("hybrid", {"quantile": 0.9}),
-    ("hybrid", {"percent": 0.2}),
+    # SCOO: shared memory per block the slice size is derived from; the
+    # reference's sort_cols layout (scoo_matrix_class.cpp:102-138)
+    ("scoo", {"shared_mem": 49152}), ("scoo", {"shared_mem": 24576}), ("scoo", {"shared_mem": 98304}),
+    ("scoo", {"shared_mem": 49152, "sort_cols": True}),
+    # hybrid: ELL width at the 2/3-quantile of the row lengths, or the
+    # reference's percent rule at the percents of its sweep (main.cpp:247-279:
+    # 0, 0.35, 0.70)
+    ("hybrid", {"quantile": 2 / 3}), ("hybrid", {"percent": 0.0}), ("hybrid", {"percent": 0.35}),
+    ("hybrid", {"percent": 0.7}),
 ]
 assert len(CONFIGS) == N_OUT
 SLOT_AVAILABLE = np.array([c is not None for c in CONFIGS])
@@ -91,19 +95,37 @@ def admissible(m: csr_matrix_class) -> np.ndarray:
     for i in range(24, 28):
         if hybrid_width(m, CONFIGS[i][1]) * m.rows * vs > ELL_MAX_BYTES:
             ok[i] = False
+    if m.nnz == 0:
+        ok[23] = False  # the sort_cols layout needs elements
     return ok
 
 
-def build_slot(m: csr_matrix_class, i: int, sm_count: int):
-    """DeviceMatrix for slot i (host conversion + upload)."""
+def build_slot(m: csr_matrix_class, i: int, sm_count: int, dev_csr=None):
+    """DeviceMatrix for slot i.  With dev_csr (device row_ptr, columns, values
+    of m) the layout is converted on the GPU (mfp_matrix_create_device, the
+    same arrays as the host converters); otherwise on the host, then uploaded."""
     from .device import FORMAT_NAMES, DeviceMatrix
     from .formats import hybrid_matrix_class, scoo_matrix_class
     name, cfg = CONFIGS[i]
     fmt = FORMAT_NAMES[name]
+    if dev_csr is not None:
+        rp, ci, va = dev_csr
+        if name.startswith("csr"):
+            return DeviceMatrix.from_device_csr(rp, ci, va, m.cols, fmt, config=cfg or None)
+        if name == "scoo":
+            prm = _capi.ScooParams()
+            call("mfp_scoo_params_compute", m.rows, sm_count, cfg["shared_mem"], 1 if m.dtype == np.float64 else 0,
+                 C.byref(prm))
+            return DeviceMatrix.from_device_csr(rp, ci, va, m.cols, fmt, scoo=prm,
+                                                scoo_sort_cols=bool(cfg.get("sort_cols")))
+        if name == "hybrid":
+            return DeviceMatrix.from_device_csr(rp, ci, va, m.cols, fmt, ell_width=hybrid_width(m, cfg))
+        return DeviceMatrix.from_device_csr(rp, ci, va, m.cols, fmt)
     if name.startswith("csr"):
         return DeviceMatrix.from_csr(m, fmt, cfg or None)
     if name == "scoo":
-        return DeviceMatrix.from_scoo(scoo_matrix_class(sm_count, cfg["shared_mem"], m))
+        return DeviceMatrix.from_scoo(scoo_matrix_class(sm_count, cfg["shared_mem"], m,
+                                                        sort_cols=bool(cfg.get("sort_cols"))))
     if name == "hybrid":
         hm = hybrid_matrix_class(m)
         hm.allocate_width(m, hybrid_width(m, cfg))
@@ -120,10 +142,14 @@ def sweep(m: csr_matrix_class, reps: int = 5, sm_count: int = 148, slots=None) -
     x = torch.ones(max(1, m.cols), dtype=torch.float32 if m.data.dtype == np.float32 else torch.float64,
                    device="cuda")
     y = torch.empty(max(1, m.rows), dtype=x.dtype, device="cuda")
+    dev_csr = None
+    if m.nnz:  # one upload; every layout is converted from it on the GPU
+        dev_csr = (torch.from_numpy(m.row_ptr.view(np.int32)).cuda(), torch.from_numpy(m.columns.view(np.int32)).cuda(),
+                   torch.from_numpy(m.data).cuda())
     for i in (slots if slots is not None else range(N_OUT)):
         if not ok[i]:
             continue
-        dm = build_slot(m, i, sm_count)
+        dm = build_slot(m, i, sm_count, dev_csr)
         try:
             _, med = dm.time(x, y, reps=reps, flush_l2=True)
             t[i] = med
@@ -287,7 +313,7 @@ def regret(times: np.ndarray, chosen: np.ndarray) -> np.ndarray:
 FAMILIES = ("uniform", "zipf", "banded", "block_diagonal", "stencil", "dense_rows")
 
 
-def family_matrix(seed: int, nnz_cap: int = 1 << 21, rows_lo: int = 10_000, rows_hi: int = 10_000_000):
+def family_matrix(seed: int, nnz_cap: int = 1 << 22, rows_lo: int = 10_000, rows_hi: int = 10_000_000):
     """One seeded matrix: rows log-uniform in [rows_lo, rows_hi], mean row
     length log-uniform in [2, 256], family uniform among FAMILIES (Zipf alpha
     in [1.5, 3], dense rows up to 1e5 nonzeros); rows are reduced to keep

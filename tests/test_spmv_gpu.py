@@ -162,6 +162,19 @@ def test_long_rows_split_and_repeatable(oracle_lib, dt, fmt):
     assert np.array_equal(ys[0], ys[1]) and np.array_equal(ys[1], ys[2])
 
 
+@pytest.mark.parametrize("name", ["laplacian_512", "power_law_300k", "stencil_40", "banded_200k", "uniform_rect"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE])
+def test_warp_tile_csr_kernel(oracle_lib, name, dt, fmt):
+    """kernel 4: 256 consecutive elements per warp, rows from row_ptr, the COO
+    reduction and fix-up; repeatable bit for bit."""
+    m = syn(name).astype(dt)
+    x = synth.vector(5, m.cols).astype(dt)
+    ys = run(m, fmt, x, {"kernel": 4}, reps=2)
+    check_tol(oracle_lib, m, x, ys[0], f"{name}/{dt.__name__}/tile fmt{fmt}")
+    assert np.array_equal(ys[0], ys[1])
+
+
 @pytest.mark.parametrize("lanes", [2, 4, 8, 16, 32])
 def test_vector_lane_counts(oracle_lib, lanes):
     m = syn("power_law_300k").astype(np.float32)
@@ -170,7 +183,7 @@ def test_vector_lane_counts(oracle_lib, lanes):
 
 
 @pytest.mark.parametrize("cfg", [{"long_row_threshold": 300, "piece_nnz": 256}, {"assist_threshold": 8},
-                                 {"bin_nnz": 64}, {"bin_nnz": 700, "long_row_threshold": 5000}])
+                                 {"bin_nnz": 64}, {"bin_nnz": 700, "long_row_threshold": 5000}, {"kernel": 4}])
 @pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE])
 def test_csr_plan_configurations(oracle_lib, cfg, fmt):
     m = _long_rows_matrix(np.float64)
@@ -300,6 +313,27 @@ def test_host_buffer_call_equals_device_call(fmt):
     assert np.array_equal(y_host, yt.cpu().numpy())
     info = dm.info()
     assert info.nnz == m.nnz and info.algorithmic_bytes == m.nnz * 8 + (m.rows + 1) * 4 + m.cols * 4 + m.rows * 4
+
+
+@pytest.mark.parametrize("fmt", ALL)
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_host_call_with_page_locked_buffers(fmt, dt):
+    """Page-locked host y: formats that store rows in order write it directly
+    (no copy-out); the result equals the device-buffer call bit for bit."""
+    m = syn("stencil_40").astype(dt)
+    x = synth.vector(8, m.cols).astype(dt)
+    dm = DeviceMatrix.build(m, fmt, hybrid_width=27)
+    hx = torch.from_numpy(x).pin_memory().numpy()
+    hy_t = torch.full((m.rows,), float("nan"), dtype=torch.from_numpy(x[:1]).dtype).pin_memory()
+    hy = hy_t.numpy()
+    for _ in range(2):
+        dm.spmv_host(hx, hy)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty(m.rows, dtype=xt.dtype, device="cuda")
+    dm.spmv(xt, yt)
+    torch.cuda.synchronize()
+    assert np.array_equal(hy, yt.cpu().numpy())
+    dm.close()
 
 
 @pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, COO, SCOO, HYBRID])
