@@ -352,6 +352,21 @@ def measure_load_ceiling(m, steps, warmup, flush, stream, peak, best_ms):
             res[key]["stream_gbs"] = round(m.nnz * 8 / (ms * 1e-3) / 1e9, 1)
         if mode != 0:
             res[key]["gathers_per_ms"] = round(m.nnz / ms / 1e6, 1)
+    # where the gather limit sits: the same gathers held in L1 (16 KB of x),
+    # and gathers through TMA tile::gather4 (all of them, or half beside ld)
+    time_launches(probe(3, 0), warmup, flush, stream)
+    ms = statistics.median(time_launches(probe(3, 0), steps, flush, stream))
+    res["gather_l1_resident"] = {"ms": round(ms, 5), "gathers_per_ms": round(m.nnz / ms / 1e6, 1)}
+
+    def probe4(mode):
+        return lambda: call("mfp_probe_spmv_gather4", mode, m.nnz, m.cols, C.c_void_p(ci.data_ptr()),
+                            C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), out.numel(), s)
+    for key, mode in (("gather_tma_gather4", 4), ("gather_half_tma_half_ld", 5)):
+        time_launches(probe4(mode), warmup, flush, stream)
+        ms = statistics.median(time_launches(probe4(mode), steps, flush, stream))
+        n = m.nnz // 256 * 256
+        res[key] = {"ms": round(ms, 5), "gathers_per_ms": round(n / ms / 1e6, 1),
+                    "error_ctas": int(torch.isnan(out[:4096]).sum().item())}
     floor = min(res[k]["ms"] for k in ("loads_ldg", "loads_l2_only", "loads_no_l1_allocate"))
     nbytes = algorithmic_bytes(m.rows, m.cols, m.nnz)
     res["floor_ms"] = floor
@@ -360,7 +375,7 @@ def measure_load_ceiling(m, steps, warmup, flush, stream, peak, best_ms):
     res["best_format_ms"] = best_ms
     res["best_format_over_floor"] = round(best_ms / floor, 3)
     res["note"] = ("loads of an SpMV without the rows (values + column ids streamed, x gathered); units: "
-                   "gathers_per_ms in millions")
+                   "gathers_per_ms in millions; gather_l1_resident folds every gather into 16 KB of x")
     return res
 
 

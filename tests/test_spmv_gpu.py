@@ -254,6 +254,34 @@ def test_coo_drops_row_ids_beyond_rows(oracle_lib, nnz_valid):
     assert np.all(np.abs(got[:rows].astype(np.float64) - ys) <= 1e-5 * ab)
 
 
+@pytest.mark.parametrize("name", ["power_law_300k", "stencil_40"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_raw_hybrid_entry_point_matches_handle(oracle_lib, name, dt):
+    """mfp_hybrid_spmv_* on the reference layout (the ELL kernel, then the COO
+    passes adding the tail) against the oracle and the handle's one-pass kernel."""
+    m = syn(name).astype(dt)
+    x = synth.vector(12, m.cols).astype(dt)
+    w = F.row_length_quantile(m, 2 / 3)
+    hm = F.hybrid_matrix_class(m)
+    hm.allocate_width(m, w)
+    e, c = hm.ell_matrix, hm.coo_matrix
+    dv = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()  # noqa: E731
+    d_ed, d_ec, d_cd, d_cc, d_cr, d_x = (dv(a) for a in (e.data, e.columns, c.data, c.cols_, c.rows_, x))
+    nb = C.c_size_t()
+    call("mfp_hybrid_workspace_bytes", m.rows, c.elements_count, C.byref(nb))
+    ws = torch.empty(max(1, nb.value), dtype=torch.uint8, device="cuda")
+    y = torch.full((m.rows,), float("nan"), dtype=d_x.dtype, device="cuda")
+    fn = "mfp_hybrid_spmv_f32" if dt == np.float32 else "mfp_hybrid_spmv_f64"
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    call(fn, m.rows, m.cols, w, p(d_ed), p(d_ec), c.elements_count, p(d_cd), p(d_cc), p(d_cr), p(d_x), p(y), p(ws),
+         nb.value, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    y_raw = y.cpu().numpy()
+    check_tol(oracle_lib, m, x, y_raw, f"raw hybrid {name}")
+    y_handle = run(m, HYBRID, x, hybrid_width=w)
+    check_tol(oracle_lib, m, x, y_handle, f"one-pass hybrid {name}")
+
+
 def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
     m = syn("power_law_300k").astype(np.float32)
     x = synth.vector(4, m.cols).astype(np.float32)
