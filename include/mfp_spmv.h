@@ -542,11 +542,6 @@ int mfp_matrix_create_scoo(int value_type, uint32_t rows, uint32_t cols, uint32_
                            const mfp_scoo_params *params, const uint32_t *c_index,
                            const uint32_t *r_index, const uint32_t *slices_ptr,
                            const void *values, mfp_matrix **out);
-/* Hybrid handles (this one and mfp_matrix_create_device) keep the ELL part
- * and the row-sorted COO tail, and also index the tail by 256-row block (each
- * element's row as a one-byte offset in its block, the blocks' tail ranges):
- * mfp_matrix_spmv then runs one kernel per call in which each CTA sums its
- * rows' ELL slots and its block's tail and writes y once. */
 int mfp_matrix_create_hybrid(int value_type, uint32_t rows, uint32_t cols, uint32_t ell_width,
                              const uint32_t *ell_columns, const void *ell_data, uint32_t coo_nnz,
                              const uint32_t *coo_rows, const uint32_t *coo_cols,

@@ -15,8 +15,9 @@
    at the configuration's full sizes (seeds 2,000,000 + i, nonzeros up to
    --big-cap) on which the selector is judged as is and with its sweep
    fallback for features outside the training range.
-2. Training: the MLP 12-64-64-28 on the engine's CUDA kernels (Adam, masked
-   MSE on log(time / best)).
+2. Training: an ensemble of MLPs 12-64-64-28 (--members, seeds 0, 1, ...)
+   on the engine's CUDA kernels (Adam, masked MSE on log(time / best)); the
+   selector averages the members' outputs.
 3. Regret on the held-out matrices: time of the selected configuration /
    best time.  Reported beside it:
    - the method without the network: the single configuration that is best
@@ -100,6 +101,7 @@ def main() -> None:
     ap.add_argument("--out", default="selector_out")
     ap.add_argument("--dataset", default=None)
     ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--members", type=int, default=10)
     a = ap.parse_args()
     import torch
 
@@ -126,7 +128,7 @@ def main() -> None:
                             sweep_s_big=sweep_bg, nnz_cap=np.array([a.cap, a.big_cap]),
                             slots=np.array([S.config_label(i) for i in range(S.N_OUT)]))
     t0 = time.time()
-    sel = S.train(Ftr, Ttr, epochs=a.epochs)
+    sel = S.train(Ftr, Ttr, epochs=a.epochs, members=a.members)
     train_s = time.time() - t0
     sel.save(out / "selector_weights.npz")
 
@@ -150,7 +152,8 @@ def main() -> None:
     per_family = {f: summary(r[fam_te == f]) for f in sorted(set(fam_te.tolist()))}
     best_slots = np.bincount(np.argmin(np.where(ok_te, Tte, np.inf), axis=1), minlength=S.N_OUT)
     res = {"config": "learned_selector", "train_matrices": int(len(Ftr)), "held_out_matrices": int(len(Fte)),
-           "network": "MLP 12-64-64-28 FP32, trained with mfp_mlp_forward/backward/adam",
+           "network": f"ensemble of {a.members} MLPs 12-64-64-28 FP32 (outputs averaged), trained with "
+                      "mfp_mlp_forward/backward/adam",
            "epochs": a.epochs, "train_seconds": train_s, "final_train_loss": float(sel.history[-1]),
            "selector": summary(r), "selector_with_sweep_fallback": {**summary(r_fallback),
                                                                    "fallback_matrices": int((~in_range).sum())},

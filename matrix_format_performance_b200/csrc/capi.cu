@@ -1158,12 +1158,6 @@ struct mfp_matrix {
   uint32_t *base = nullptr;
   bool rows_unsorted = false;         // SCOO in the sort_cols layout
   bool long_rows = false;             // reduced-precision CSR: a row longer than kLowpTmaMaxRow
-  // hybrid, one-pass kernel: per 256-row block the first tail element, each
-  // tail element's row offset in its block, and the blocks heaviest first
-  uint32_t *tptr = nullptr;
-  uint8_t *trow8 = nullptr;
-  uint32_t *hyb_order = nullptr;
-  uint32_t hyb_blocks = 0;
 };
 
 namespace {
@@ -1204,33 +1198,6 @@ int finish_matrix(mfp_matrix *m, mfp_matrix **out) {
 }
 bool valid_vt(int vt) { return vt == MFP_F32 || vt == MFP_F64; }
 
-// The one-pass hybrid's tail index, built on the GPU from the device tail
-// rows (m->rows2): row offsets, per-block tail ranges, and the launch order
-// (blocks by tail length, heaviest first, from the ranges brought back).
-int hybrid_fused_prepare(mfp_matrix *m) {
-  m->hyb_blocks = ceil_div(m->rows, d::kBlock);
-  int st;
-  if ((st = track(m, &m->tptr, (size_t)m->hyb_blocks + 1)) || (st = track(m, &m->trow8, (size_t)m->coo_nnz)) ||
-      (st = track(m, &m->hyb_order, (size_t)m->hyb_blocks)))
-    return st;
-  const uint64_t work = std::max<uint64_t>(m->coo_nnz, (uint64_t)m->hyb_blocks + 1);
-  const uint32_t grid = (uint32_t)std::min<uint64_t>(ceil_div(work, 256), 148u * 8u);
-  d::hyb_tail_index_kernel<<<grid, 256>>>(m->coo_nnz, m->rows2, m->hyb_blocks, m->trow8, m->tptr);
-  CUDA_TRY(cudaGetLastError(), "hyb_tail_index_kernel launch");
-  std::vector<uint32_t> tp((size_t)m->hyb_blocks + 1), order(m->hyb_blocks);
-  CUDA_TRY(cudaMemcpy(tp.data(), m->tptr, tp.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost), "cudaMemcpy tptr");
-  for (uint32_t b = 0; b < m->hyb_blocks; ++b) order[b] = b;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](uint32_t a, uint32_t b) { return tp[a + 1] - tp[a] > tp[b + 1] - tp[b]; });
-  CUDA_TRY(cudaMemcpy(m->hyb_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
-           "cudaMemcpy order");
-  // what the one-pass kernel moves: ELL slots, tail values / ids / offsets,
-  // the block ranges, x and y
-  const size_t vs = value_size(m->value_type);
-  m->format_bytes = (uint64_t)m->rows * m->width * (vs + 4) + (uint64_t)m->coo_nnz * (vs + 5) +
-                    ((uint64_t)m->hyb_blocks + 1) * 4 + (uint64_t)m->cols * vs + (uint64_t)m->rows * vs;
-  return ok();
-}
 int track_bytes(mfp_matrix *m, void **p, size_t bytes) {
   unsigned char *q = nullptr;
   const int st = track(m, &q, bytes);
@@ -1475,10 +1442,6 @@ int mfp_matrix_create_hybrid(int vt, uint32_t rows, uint32_t cols, uint32_t widt
     mfp_matrix_destroy(m);
     return fail(MFP_ERROR_CUDA, "cudaMemset workspace");
   }
-  if ((st = hybrid_fused_prepare(m))) {
-    mfp_matrix_destroy(m);
-    return st;
-  }
   return finish_matrix(m, out);
 }
 
@@ -1572,7 +1535,6 @@ int mfp_matrix_create_device(int format, int vt, uint32_t rows, uint32_t cols, u
         return bail(st);
       m->ws = ws;
       if (ws && cudaMemset(ws, 0, m->ws_bytes) != cudaSuccess) return bail(fail(MFP_ERROR_CUDA, "cudaMemset workspace"));
-      if (hyb && (st = hybrid_fused_prepare(m))) return bail(st);
       break;
     }
     case MFP_FORMAT_SCOO: {
@@ -1716,7 +1678,7 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
   if (m->format == MFP_FORMAT_COO)
     out->kernel_launches = m->nnz ? 2u : (m->rows ? 1u : 0u);
   else if (m->format == MFP_FORMAT_HYBRID)
-    out->kernel_launches = 1u;  // the one-pass kernel
+    out->kernel_launches = 1u + (m->coo_nnz ? (m->coo_nnz > d::kWarpTile ? 2u : 1u) : 0u);
   else if (m->plan && m->plan->tile)  // CSR vector on short rows: warp pass + fix-up
     out->kernel_launches = 2u;
   else
@@ -1724,24 +1686,6 @@ int mfp_matrix_get_info(const mfp_matrix *m, mfp_matrix_info *out) {
   return ok();
 }
 
-}  // extern "C"
-// The one-pass hybrid (handles): ELL part and the block's tail in one kernel.
-template <typename T>
-int hyb_fused_spmv(const mfp_matrix *m, const T *x, T *y, void *stream) {
-  if (m->rows == 0) return ok();
-  if (!y || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
-  cudaStream_t s = as_stream(stream);
-  const bool vec = aligned16(m->vals2) && aligned16(m->cols2) && (reinterpret_cast<uintptr_t>(m->trow8) % 8 == 0);
-  const T *ev = static_cast<const T *>(m->vals), *tv = static_cast<const T *>(m->vals2);
-  if (vec)
-    d::hyb_fused_kernel<T, true><<<m->hyb_blocks, d::kBlock, 0, s>>>(m->rows, m->width, ev, m->cols_a, m->tptr, tv,
-                                                                    m->cols2, m->trow8, m->hyb_order, x, y);
-  else
-    d::hyb_fused_kernel<T, false><<<m->hyb_blocks, d::kBlock, 0, s>>>(m->rows, m->width, ev, m->cols_a, m->tptr, tv,
-                                                                     m->cols2, m->trow8, m->hyb_order, x, y);
-  return check_launch("hyb_fused_kernel launch");
-}
-extern "C" {
 int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
   if (!m || !y || (!x && m->cols)) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
   const bool f64 = m->value_type == MFP_F64;
@@ -1777,8 +1721,12 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                  : scoo_spmv<float>(m->rows, m->slices, m->slice_size, (const float *)m->vals, m->cols_a, m->rows_a,
                                     m->aux, m->win, m->max_window, m->order, (const float *)x, (float *)y, stream);
     case MFP_FORMAT_HYBRID:
-      return f64 ? hyb_fused_spmv<double>(m, (const double *)x, (double *)y, stream)
-                 : hyb_fused_spmv<float>(m, (const float *)x, (float *)y, stream);
+      return f64 ? hyb_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, m->coo_nnz,
+                                    (const double *)m->vals2, m->cols2, m->rows2, (const double *)x, (double *)y,
+                                    m->ws, m->ws_bytes, stream)
+                 : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
+                                   (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
+                                   m->ws_bytes, stream);
     case MFP_FORMAT_ELL_LOWP:
       return lowp_ell_spmv(m->lowp_vt, m->rows, m->cols, m->width, (const uint16_t *)m->vals, m->scale,
                            m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);
@@ -1802,11 +1750,10 @@ static bool writes_y_in_row_order(const mfp_matrix *m) {
     case MFP_FORMAT_SCOO:
     case MFP_FORMAT_CSR_LOWP:
     case MFP_FORMAT_ELL_LOWP:
-    case MFP_FORMAT_HYBRID:  // the one-pass kernel
       return !(m->plan && m->plan->tile) && !m->rows_unsorted;
     case MFP_FORMAT_CSR_VECTOR:
       return !(m->plan && m->plan->tile);
-    default:  // COO and the warp-tile kernels write rows as their tiles finish
+    default:  // COO and the warp-tile kernels write rows as their tiles finish; the hybrid adds into y
       return false;
   }
 }

@@ -1483,140 +1483,6 @@ __global__ void __launch_bounds__(kBlock) scoo_unsorted_kernel(uint32_t n_rows, 
   for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
 }
 
-// ---------------------------------------------------------------------------
-// Hybrid in one pass (handles).  CTA b owns rows [256 b, 256 b + 256): thread
-// t sums row r0 + t's ELL slots in slot order (the ell_kernel sum); the CTA
-// then reduces the block's tail elements [tptr[b], tptr[b + 1]) -- row-sorted,
-// each with its row stored as a one-byte offset in the block -- in chunks of
-// 2048 (8 per thread in registers, the CTA-wide segmented scan) into
-// shared-memory row sums, and writes y once: ELL part + tail part.  One
-// launch, no read-modify-write of y, 4 + 4 + 1 bytes per tail element instead
-// of COO's 4 + 4 + 4.  Blocks start heaviest first (`order`).
-// ---------------------------------------------------------------------------
-struct rows_u8 {
-  const uint8_t *__restrict__ p;
-  __device__ __forceinline__ uint32_t operator()(uint32_t e) const { return __ldg(p + e); }
-};
-
-__device__ __forceinline__ uint2 ld_stream8_bytes(const uint8_t *p, uint64_t pol) {
-  uint2 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
-               : "=r"(v.x), "=r"(v.y)
-               : "l"(p), "l"(pol));
-  return v;
-}
-
-// Elements [g, g + 8) of a tail chunk [c0, c1): products and row offsets.
-template <typename T, bool VEC>
-__device__ __forceinline__ uint32_t load_tail_group(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
-                                                    const uint8_t *__restrict__ rofs, const T *__restrict__ x,
-                                                    uint32_t g, uint32_t c0, uint32_t c1, T (&p)[kEpt],
-                                                    uint32_t (&r)[kEpt], uint32_t &i0, uint64_t pol) {
-  i0 = max(g, c0);
-  const uint32_t i1 = min(g + kEpt, c1);
-  if (i0 >= i1) return 0u;
-  const uint32_t cnt = i1 - i0;
-  if (VEC && cnt == kEpt) {  // i0 == g, a multiple of 8: values / ids 16-byte and offsets 8-byte aligned
-    T v0[4], v1[4];
-    uint32_t k0[4], k1[4];
-    ld_stream4(vals + i0, v0, pol);
-    ld_stream4(vals + i0 + 4, v1, pol);
-    ld_stream4(cols + i0, k0, pol);
-    ld_stream4(cols + i0 + 4, k1, pol);
-    const uint2 ro = ld_stream8_bytes(rofs + i0, pol);
-    T x0[4], x1[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      x0[k] = ld_x(x + k0[k]);
-      x1[k] = ld_x(x + k1[k]);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      p[k] = mul_rn(v0[k], x0[k]);
-      p[4 + k] = mul_rn(v1[k], x1[k]);
-      r[k] = (ro.x >> (8 * k)) & 0xffu;
-      r[4 + k] = (ro.y >> (8 * k)) & 0xffu;
-    }
-  } else {
-#pragma unroll
-    for (uint32_t k = 0; k < kEpt; ++k) {
-      if (k < cnt) {
-        const uint32_t e = i0 + k;
-        r[k] = __ldg(rofs + e);
-        p[k] = mul_rn(ld_stream1(vals + e, pol), ld_x(x + ld_stream1(cols + e, pol)));
-      }
-    }
-  }
-  return cnt;
-}
-
-template <typename T, bool VEC>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
-    hyb_fused_kernel(uint32_t n_rows, uint32_t width, const T *__restrict__ ell_v, const uint32_t *__restrict__ ell_c,
-                     const uint32_t *__restrict__ tptr, const T *__restrict__ tv, const uint32_t *__restrict__ tc,
-                     const uint8_t *__restrict__ tr, const uint32_t *__restrict__ order, const T *__restrict__ x,
-                     T *__restrict__ y) {
-  __shared__ seg_scan_smem<T> scan;
-  __shared__ T acc[kBlock];
-  const uint64_t pol = policy_evict_first();
-  const uint32_t b = order ? order[blockIdx.x] : blockIdx.x;
-  const uint32_t r0 = b * kBlock;
-  if (r0 >= n_rows) return;
-  const uint32_t nr = min((uint32_t)kBlock, n_rows - r0);
-  const uint32_t t = threadIdx.x;
-  const uint32_t eb = tptr[b], ee = tptr[b + 1];
-  acc[t] = -T(0);  // -0 + s == s for every s, so rows without tail keep their ELL sum's bits
-  // the first tail chunk's loads and gathers go out before the ELL part's
-  uint32_t c0 = eb, base8 = eb & ~7u;
-  uint32_t c1 = min(ee, base8 + (uint32_t)kChunk);
-  T pr[kEpt];
-  uint32_t rw[kEpt], i0 = 0;
-  uint32_t cnt = load_tail_group<T, VEC>(tv, tc, tr, x, base8 + t * kEpt, c0, c1, pr, rw, i0, pol);
-  T e = T(0);
-  if (t < nr) {
-    const size_t stride = n_rows;
-#pragma unroll 4
-    for (uint32_t k = 0; k < width; ++k) {
-      const size_t o = k * stride + r0 + t;
-      e = add_rn(e, mul_rn(ld_stream1(ell_v + o, pol), ld_x(x + ld_stream1(ell_c + o, pol))));
-    }
-  }
-  __syncthreads();  // acc[] initialised before any emit
-  auto emit = [&](uint32_t row, T total, bool, bool) { acc[row] = add_rn(acc[row], total); };
-  auto gap = [](uint32_t, uint32_t) {};
-  while (c0 < ee) {
-    // a chunk's emits land before the next chunk's scan barriers, which every
-    // thread passes only after its own emits
-    block_segmented_reduce_regs<T>(pr, rw, cnt, i0, c0, c1, rows_u8{tr}, emit, gap, scan);
-    c0 = c1;
-    if (c0 >= ee) break;
-    base8 = c0 & ~7u;
-    c1 = min(ee, base8 + (uint32_t)kChunk);
-    cnt = load_tail_group<T, VEC>(tv, tc, tr, x, base8 + t * kEpt, c0, c1, pr, rw, i0, pol);
-  }
-  __syncthreads();
-  if (t < nr) y[r0 + t] = add_rn(e, acc[t]);
-}
-
-// The fused hybrid's tail index from the row-sorted tail rows: each element's
-// row offset in its 256-row block, and per block the first tail element
-// (tptr[b] = first e with rows[e] >= 256 b, b = 0 .. n_blocks).
-__global__ void hyb_tail_index_kernel(uint32_t cnnz, const uint32_t *__restrict__ rows, uint32_t n_blocks,
-                                      uint8_t *__restrict__ rofs, uint32_t *__restrict__ tptr) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cnnz; i += stride)
-    rofs[i] = (uint8_t)(rows[i] & 0xffu);
-  for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b <= n_blocks; b += stride) {
-    const uint64_t key = b * kBlock;
-    uint32_t lo = 0, hi = cnnz;
-    while (lo < hi) {
-      const uint32_t mid = lo + (hi - lo) / 2u;
-      if ((uint64_t)rows[mid] < key) lo = mid + 1u; else hi = mid;
-    }
-    tptr[b] = lo;
-  }
-}
-
 template <typename T>
 __global__ void fill_kernel(uint64_t n, T *v, T value) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)

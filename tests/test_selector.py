@@ -144,7 +144,8 @@ def test_training_fits_a_learnable_rule():
     times[F[:, 0] > 0.5, 4] = 0.3
     times[F[:, 1] < -0.5, 16] = 0.2
     times[(F[:, 0] <= 0.5) & (F[:, 1] >= -0.5), 8] = 0.4
-    sel = S.train(F[:1000], times[:1000], epochs=300, batch=128, lr=3e-3)
+    sel = S.train(F[:1000], times[:1000], epochs=300, batch=128, lr=3e-3, members=2)
+    assert sel.params.shape[0] == 2  # two members, outputs averaged
     assert sel.history[-1] < 0.25 * sel.history[0]
     ok = np.isfinite(times[1000:])
     chosen = sel.choose(F[1000:], ok)
@@ -163,6 +164,12 @@ def _held_out():
     return d, w
 
 
+def ensemble_forward(w, F):
+    """The committed ensemble with the NumPy network: members' outputs averaged."""
+    x = (F - w.mu) / w.sigma
+    return np.mean([ref_forward(p, x)[2] for p in w.params], axis=0)
+
+
 def test_committed_selector_meets_target_on_cpu_reference():
     """The committed weights, evaluated with the NumPy network on the
     committed held-out measurements: >= 90% of the held-out matrices get a
@@ -171,7 +178,7 @@ def test_committed_selector_meets_target_on_cpu_reference():
     d, w = _held_out()
     F, T = d["F_test"].astype(np.float64), d["T_test"].astype(np.float64)
     assert len(F) == 200 and len(d["F_train"]) == 2000
-    _, _, y = ref_forward(w.params, (F - w.mu) / w.sigma)
+    y = ensemble_forward(w, F)
     chosen = np.where(np.isfinite(T), y, np.inf).argmin(axis=1)
     r = S.regret(T, chosen)
     assert np.mean(r <= 1.05) >= 0.9
@@ -191,7 +198,7 @@ def test_committed_selector_cuda_forward_agrees():
     F, T = d["F_test"], d["T_test"].astype(np.float64)
     ok = np.isfinite(T)
     g = w.choose(F, ok)
-    _, _, y = ref_forward(w.params, (F.astype(np.float64) - w.mu) / w.sigma)
+    y = ensemble_forward(w, F.astype(np.float64))
     c = np.where(ok, y, np.inf).argmin(axis=1)
     assert np.mean(g == c) >= 0.99
     assert np.mean(S.regret(T, g) <= 1.05) >= 0.9
@@ -201,8 +208,9 @@ def test_committed_selector_cuda_forward_agrees():
 def test_select_end_to_end_and_sweep_fallback():
     """select() on a fresh matrix returns an admissible configuration; a matrix
     outside the training range goes to the exhaustive sweep."""
-    _, w = _held_out()
-    m, _ = S.family_matrix(4_000_000)
+    d, w = _held_out()
+    cap = int(d["nnz_cap"][0]) if "nnz_cap" in d.files else 1 << 21  # the training set's size cap
+    m, _ = S.family_matrix(4_000_000, nnz_cap=cap)
     slot, how = w.select(m)
     assert how == "predicted" and S.admissible(m)[slot]
     tiny = synth.uniform(50, 1, 3, seed=1).astype(np.float32)  # 50 rows: below the training range

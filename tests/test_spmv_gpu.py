@@ -258,7 +258,8 @@ def test_coo_drops_row_ids_beyond_rows(oracle_lib, nnz_valid):
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
 def test_raw_hybrid_entry_point_matches_handle(oracle_lib, name, dt):
     """mfp_hybrid_spmv_* on the reference layout (the ELL kernel, then the COO
-    passes adding the tail) against the oracle and the handle's one-pass kernel."""
+    passes adding the tail) against the oracle, and the handle on the same
+    layout."""
     m = syn(name).astype(dt)
     x = synth.vector(12, m.cols).astype(dt)
     w = F.row_length_quantile(m, 2 / 3)
@@ -279,7 +280,7 @@ def test_raw_hybrid_entry_point_matches_handle(oracle_lib, name, dt):
     y_raw = y.cpu().numpy()
     check_tol(oracle_lib, m, x, y_raw, f"raw hybrid {name}")
     y_handle = run(m, HYBRID, x, hybrid_width=w)
-    check_tol(oracle_lib, m, x, y_handle, f"one-pass hybrid {name}")
+    check_tol(oracle_lib, m, x, y_handle, f"hybrid handle {name}")
 
 
 def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
