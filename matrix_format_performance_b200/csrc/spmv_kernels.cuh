@@ -902,25 +902,53 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
   }
   const uint32_t base = a & ~3u;
   for (uint32_t i = t; i <= nrows && i <= (uint32_t)kBlock; i += kBlock) sm.m.rp[i] = A.row_ptr[rb + i];
+  if (t == 0) sm.m.nassist = 0u;
   if (b > a) stage<T, VEC, false>(A.vals, A.cols, nullptr, x_global<T>{A.x}, a, b, sm.m.prod, nullptr, pol);
   __syncthreads();
+  // Rows are summed by power-of-two lane groups (one thread per row once the
+  // bin holds more than 128 rows); a row longer than the assist threshold
+  // that would get fewer than 32 lanes is queued for a whole warp instead, so
+  // one long row does not hold up its CTA.  A row's sum order depends only on
+  // its length and position, so results repeat bit for bit.
+  // (at least 9 elements per queued row: a bin's <= 2044 elements queue at
+  // most 227 rows, within the 256-entry list)
+  const uint32_t athr = max(A.assist_thr, 8u);
+  uint32_t tpr = 1;
   if (nrows <= (uint32_t)kBlock) {
-    uint32_t tpr = kBlock / nrows;  // >= 1
+    tpr = kBlock / nrows;  // >= 1
     tpr = tpr >= 32 ? 32u : (1u << (31 - __clz(tpr)));
     const uint32_t grp = t / tpr, lane = t % tpr;
     T acc = T(0);
-    const bool valid = grp < nrows;
+    bool valid = grp < nrows;
     if (valid) {
       const uint32_t s = sm.m.rp[grp], e = sm.m.rp[grp + 1];
-      if (s < e) acc = strided_sum(sm.m.prod, s - base, e - base, lane, tpr);
+      if (tpr < 32 && e - s > athr) {
+        valid = false;
+        if (lane == 0) sm.m.assists[atomicAdd(&sm.m.nassist, 1u)] = grp;
+      } else if (s < e) {
+        acc = strided_sum(sm.m.prod, s - base, e - base, lane, tpr);
+      }
     }
     acc = group_reduce_down(acc, (int)tpr);
     if (valid && lane == 0) A.y[rb + grp] = acc;
   } else {
     for (uint32_t r = t; r < nrows; r += kBlock) {
       const uint32_t s = A.row_ptr[rb + r], e = A.row_ptr[rb + r + 1];
-      A.y[rb + r] = s < e ? seq_sum(T(0), sm.m.prod, s - base, e - base) : T(0);
+      if (e - s > athr)
+        sm.m.assists[atomicAdd(&sm.m.nassist, 1u)] = r;
+      else
+        A.y[rb + r] = s < e ? seq_sum(T(0), sm.m.prod, s - base, e - base) : T(0);
     }
+  }
+  if (tpr == 32) return;  // whole warps already
+  __syncthreads();
+  const uint32_t nas = sm.m.nassist, lane = t & 31u;
+  for (uint32_t q = t >> 5; q < nas; q += kBlock / 32) {
+    const uint32_t r = sm.m.assists[q];
+    const uint32_t s = A.row_ptr[rb + r], e = A.row_ptr[rb + r + 1];
+    T part = strided_sum(sm.m.prod, s - base, e - base, lane, 32u);
+    part = group_reduce_down(part, 32);
+    if (lane == 0) A.y[rb + r] = part;
   }
 }
 
