@@ -56,10 +56,16 @@ namespace dev {
 #ifndef MFP_CSR_MINBLOCKS64_OTHER
 #define MFP_CSR_MINBLOCKS64_OTHER 6
 #endif
-// CTAs per SM the register-resident COO / SCOO kernels are register-limited
-// to, FP32 and FP64 (FP64: 5 measured faster than 4 and 6).
+// CTAs per SM the warp-tile kernels (COO warp pass, warp-tile CSR) are
+// register-limited to in FP32: 8 (32 registers) measured fastest on the
+// power-law matrix (COO 0.169 -> 0.165 ms, CSR vector 0.187 -> 0.181 ms,
+// hybrid tail 0.175 -> 0.169 ms against 6) and the stencil; SCOO keeps 6
+// (0.195 ms against 0.203 at 8).  FP64: 5 measured faster than 4 and 6.
 #ifndef MFP_COO_MINBLOCKS
-#define MFP_COO_MINBLOCKS 6
+#define MFP_COO_MINBLOCKS 8
+#endif
+#ifndef MFP_SCOO_MINBLOCKS
+#define MFP_SCOO_MINBLOCKS 6
 #endif
 #ifndef MFP_COO_MINBLOCKS64
 #define MFP_COO_MINBLOCKS64 5
@@ -1390,7 +1396,7 @@ struct scoo_smem_static {
 };
 
 template <typename T, bool VEC, bool XWIN>
-__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : MFP_COO_MINBLOCKS64) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,
                                                       const uint32_t *__restrict__ ridx,
