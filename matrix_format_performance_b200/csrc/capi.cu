@@ -888,7 +888,7 @@ int lowp_ell_spmv(int vt, uint32_t rows, uint32_t cols_n, uint32_t width, const 
 #define MFP_LELL(VT, D16)                                                                         \
   {                                                                                               \
     d::lowp_ell_args<VT, D16> A{rows, width, cols_n, q, scale, cols, off, x, y};                  \
-    if (MFP_LOWP_XRUN && vec && D16 && aligned16(x))                                              \
+    if (MFP_LOWP_XRUN && vec && D16 && aligned16(x) && aligned16(y) && aligned16(scale))          \
       d::lowp_ell_kernel<VT, D16, true, true><<<grid, d::kBlock, 0, s>>>(A);                      \
     else if (vec)                                                                                 \
       d::lowp_ell_kernel<VT, D16, true><<<grid, d::kBlock, 0, s>>>(A);                            \

@@ -581,9 +581,11 @@ struct lowp_ell_args {
   float *__restrict__ y;
 };
 
-// CTAs per SM the 16-bit ELL kernel is register-limited to: 8 (32 registers)
-// holds the 27-point 128^3 stencil's 1,024 CTAs in one wave on 148 SMs
-// (6, at 40 registers, left a second wave of 136 CTAs).
+// CTAs per SM the 16-bit ELL kernel (16-bit offsets, 8 rows per thread) is
+// register-limited to: 8 (32 registers) holds the 27-point 128^3 stencil's
+// 1,024 CTAs in one wave on 148 SMs (6, at 40 registers, left a second wave
+// of 136 CTAs).  The uint32-column variants keep 6 (40 registers, which they
+// need without spilling).
 #ifndef MFP_LOWP_ELL_MINBLOCKS
 #define MFP_LOWP_ELL_MINBLOCKS 8
 #endif
@@ -599,8 +601,13 @@ __device__ __forceinline__ void ld_x8_run(const float *__restrict__ x, uint32_t 
   for (int j = 0; j < 8; ++j) xv[j] = sh == 0 ? w[j] : sh == 1 ? w[j + 1] : sh == 2 ? w[j + 2] : w[j + 3];
 }
 
+// XRUN (16-bit offsets, 16-byte-aligned x, y and scale): a thread whose 8
+// rows share one offset in a slot reads their 8 consecutive x entries as
+// three 16-byte loads instead of 8 gathers, and the scales and y move 16
+// bytes at a time.  One slot is in flight, to stay within 32 registers.
 template <int VT, bool D16, bool VEC, bool XRUN = false>
-__global__ void __launch_bounds__(kBlock, MFP_LOWP_ELL_MINBLOCKS) lowp_ell_kernel(const lowp_ell_args<VT, D16> A) {
+__global__ void __launch_bounds__(kBlock, D16 && VEC ? MFP_LOWP_ELL_MINBLOCKS : 6)
+    lowp_ell_kernel(const lowp_ell_args<VT, D16> A) {
   const uint64_t pol = policy_evict_first();
   const size_t stride = A.n_rows;
   if (VEC) {
@@ -609,7 +616,7 @@ __global__ void __launch_bounds__(kBlock, MFP_LOWP_ELL_MINBLOCKS) lowp_ell_kerne
     float acc[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[j] = 0.f;
-#pragma unroll 2
+#pragma unroll(XRUN ? 1 : 2)
     for (uint32_t k = 0; k < A.width; ++k) {
       const size_t o = (size_t)k * stride + r;
       uint32_t qv[4], c[8];
@@ -626,7 +633,8 @@ __global__ void __launch_bounds__(kBlock, MFP_LOWP_ELL_MINBLOCKS) lowp_ell_kerne
         if (XRUN) {
           // the 8 rows share one offset: their columns are c[0] .. c[0] + 7
           const uint32_t d2 = (dv[0] & 0xffffu) | (dv[0] << 16);
-          run = dv[0] == d2 && dv[1] == d2 && dv[2] == d2 && dv[3] == d2 && (c[0] & ~3u) + 12u <= A.n_cols;
+          run = dv[0] == d2 && dv[1] == d2 && dv[2] == d2 && dv[3] == d2 && A.n_cols >= 12u &&
+                c[0] <= A.n_cols - 12u;  // (c[0] & ~3) + 12 <= n_cols, overflow-free
         }
       } else {
         uint32_t c0[4], c1[4];
@@ -652,8 +660,16 @@ __global__ void __launch_bounds__(kBlock, MFP_LOWP_ELL_MINBLOCKS) lowp_ell_kerne
         acc[2 * j + 1] = __fmaf_rn(f.y, xv[2 * j + 1], acc[2 * j + 1]);
       }
     }
+    if (XRUN) {  // 16-byte-aligned y and scale: r is a multiple of 8
+      const float4 s0 = __ldg(reinterpret_cast<const float4 *>(A.scale + r));
+      const float4 s1 = __ldg(reinterpret_cast<const float4 *>(A.scale + r + 4));
+      *reinterpret_cast<float4 *>(A.y + r) = make_float4(acc[0] * s0.x, acc[1] * s0.y, acc[2] * s0.z, acc[3] * s0.w);
+      *reinterpret_cast<float4 *>(A.y + r + 4) =
+          make_float4(acc[4] * s1.x, acc[5] * s1.y, acc[6] * s1.z, acc[7] * s1.w);
+    } else {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) A.y[r + j] = acc[j] * A.scale[r + j];
+      for (int j = 0; j < 8; ++j) A.y[r + j] = acc[j] * A.scale[r + j];
+    }
   } else {
     // 8 rows per thread, interleaved across the warp: row = warp base + 32 j +
     // lane, so every load and every x gather of a warp is contiguous

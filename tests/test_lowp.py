@@ -235,3 +235,36 @@ def test_lowp_ell_accuracy(oracle_lib, name, vt, index16):
     torch.cuda.synchronize()
     _check(oracle_lib, m, vt, yt.cpu().numpy(), x)
     assert dm.info().value_type == vt
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["stencil_32", "banded_100k"])
+@pytest.mark.parametrize("vt", [BF16, F16])
+def test_lowp_ell_kernel_variants_agree(oracle_lib, name, vt):
+    """The 16-bit-offset ELL kernel's three variants give the same bits: x, y
+    and scales 16-byte aligned (runs of x, 16-byte y stores), y and scales
+    shifted by 4 bytes (8 rows per thread, scalar stores), and q shifted off
+    16-byte alignment (lane-interleaved rows)."""
+    import torch
+    m = case(name)
+    assert m.rows % 8 == 0
+    w, q, idx, sc = _lowp_ell_host(m, vt, True)
+    x = synth.vector(2, m.cols).astype(np.float32)
+    keep = []
+
+    def dev(a, off):
+        t, p = _dev_copy(np.ascontiguousarray(a), off)
+        keep.append(t)
+        return C.c_void_p(p)
+
+    outs = []
+    for q_off, ys_off in ((0, 0), (0, 4), (2, 4)):
+        qd, od = dev(q, q_off), dev(idx, q_off)
+        scd, xd = dev(sc, ys_off), dev(x, 0)
+        yraw, yp = _dev_copy(np.full(m.rows, np.nan, np.float32), ys_off)
+        call("mfp_lowp_ell_spmv", vt, m.rows, m.cols, w, qd, scd, None, od, xd, C.c_void_p(yp), None)
+        torch.cuda.synchronize()
+        outs.append(yraw[ys_off:ys_off + 4 * m.rows].cpu().numpy().view(np.float32).copy())
+    for y in outs[1:]:
+        assert np.array_equal(outs[0].view(np.uint32), y.view(np.uint32))
+    _check(oracle_lib, m, vt, outs[0], x)
