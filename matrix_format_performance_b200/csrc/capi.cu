@@ -31,6 +31,13 @@ int cuda_fail(cudaError_t e, const char *what) {
   } while (0)
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline bool aligned32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
+// Per-lane group loads of the warp-tile kernels: 2 = one 32-byte load per
+// array, 1 = two 16-byte loads, 0 = element by element.
+inline int vec_level(const void *a, const void *b, const void *c = nullptr) {
+  if (aligned32(a) && aligned32(b) && (!c || aligned32(c))) return 2;
+  return aligned16(a) && aligned16(b) && (!c || aligned16(c)) ? 1 : 0;
+}
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
@@ -693,18 +700,16 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   cw.flags = reinterpret_cast<uint32_t *>(base + (size_t)n_wt * 16u);
   cw.tail_row = cw.flags + n_wt;
   const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
-  const bool vec = aligned16(data) && aligned16(cols) && aligned16(rids);
+  const int vec = vec_level(data, cols, rids);
   cudaStream_t s = as_stream(stream);
+  auto k = vec == 2 ? d::coo_warp_kernel<T, 2, ACCUM>
+                    : (vec == 1 ? d::coo_warp_kernel<T, 1, ACCUM> : d::coo_warp_kernel<T, 0, ACCUM>);
   // the accumulating warp pass (hybrid tail) follows the ELL launch of the same call
   cudaError_t e;
   if (ACCUM)
-    e = vec ? launch_after(d::coo_warp_kernel<T, true, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr)
-            : launch_after(d::coo_warp_kernel<T, false, ACCUM>, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr);
+    e = launch_after(k, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr);
   else {
-    if (vec)
-      d::coo_warp_kernel<T, true, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
-    else
-      d::coo_warp_kernel<T, false, ACCUM><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
+    k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) return cuda_fail(e, "coo_warp_kernel launch");
@@ -733,10 +738,9 @@ int csr_tile_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols,
   cw.flags = reinterpret_cast<uint32_t *>(base + (size_t)n_wt * 16u);
   cw.tail_row = cw.flags + n_wt;
   const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
-  if (aligned16(data) && aligned16(cols))
-    d::csr_tile_kernel<T, true><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rp, plan->tile_prev, x, y, cw, hdr);
-  else
-    d::csr_tile_kernel<T, false><<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rp, plan->tile_prev, x, y, cw, hdr);
+  const int vec = vec_level(data, cols);
+  auto k = vec == 2 ? d::csr_tile_kernel<T, 2> : (vec == 1 ? d::csr_tile_kernel<T, 1> : d::csr_tile_kernel<T, 0>);
+  k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rp, plan->tile_prev, x, y, cw, hdr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "csr_tile_kernel launch");
   const uint32_t fgrid = std::max(ceil_div(n_wt, d::kBlock), std::min(ceil_div(rows, d::kBlock * 8u), 148u * 4u));
@@ -745,7 +749,7 @@ int csr_tile_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols,
   return ok();
 }
 
-template <typename T, bool VEC, bool XWIN, bool UNSORTED = false>
+template <typename T, int VEC, bool XWIN, bool UNSORTED = false>
 int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32_t slice, const T *v,
                 const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
                 const uint32_t *order, const T *x, T *y) {
@@ -774,18 +778,22 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
   const size_t dyn = acc_bytes + (size_t)maxw * sizeof(T);
   if (dyn + sizeof(d::scoo_smem_static<T>) > 227 * 1024)
     return fail(MFP_ERROR_NOT_SUPPORTED, "slice_size %u / window %u too large for shared memory", slice, maxw);
-  const bool vec = aligned16(v) && aligned16(ci) && aligned16(ri);
+  const int vec = vec_level(v, ci, ri);
   cudaStream_t s = as_stream(stream);
   if (UNSORTED) {
-    if (win) return scoo_launch<T, false, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
-    return scoo_launch<T, false, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+    if (win) return scoo_launch<T, 0, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+    return scoo_launch<T, 0, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
   }
-  if (vec) {
-    if (win) return scoo_launch<T, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
-    return scoo_launch<T, true, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  if (vec == 2) {
+    if (win) return scoo_launch<T, 2, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+    return scoo_launch<T, 2, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
   }
-  if (win) return scoo_launch<T, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
-  return scoo_launch<T, false, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  if (vec == 1) {
+    if (win) return scoo_launch<T, 1, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+    return scoo_launch<T, 1, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  }
+  if (win) return scoo_launch<T, 0, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  return scoo_launch<T, 0, false>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
 }
 
 // Pipelined reduced-precision kernel: CAP elements per stage, S stages.  A

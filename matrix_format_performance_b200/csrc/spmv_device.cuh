@@ -46,6 +46,27 @@ __device__ __forceinline__ void ld_stream4(const uint32_t *p, uint32_t (&v)[4], 
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
                : "l"(p), "l"(pol));
 }
+// 32-byte streaming loads (sm_100 256-bit vectors; p 32-byte aligned): a lane
+// that reads a whole sector asks L2 for it once.  Two 16-byte loads of the
+// same sector miss in L1 twice and send two requests.
+__device__ __forceinline__ void ld_stream8(const float *p, float (&v)[8], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream8(const double *p, double (&v)[8], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f64 {%0,%1,%2,%3}, [%4], %5;"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p), "l"(pol));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f64 {%0,%1,%2,%3}, [%4], %5;"
+               : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
+               : "l"(p + 4), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream8(const uint32_t *p, uint32_t (&v)[8], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "l"(p), "l"(pol));
+}
 __device__ __forceinline__ float ld_stream1(const float *p, uint64_t pol) {
   float v;
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"

@@ -340,17 +340,28 @@ __device__ __forceinline__ void block_segmented_reduce(const T *s_prod, const ui
 // block_segmented_reduce, without staging products and row ids through
 // shared memory.
 // ---------------------------------------------------------------------------
-template <typename T, bool VEC, typename XS>
+template <typename T, int VEC, typename XS>
 __device__ __forceinline__ uint32_t load_run_group(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                                                    const uint32_t *__restrict__ rows, XS xs, uint32_t g,
                                                    uint32_t c0, uint32_t c1, T (&p)[kEpt], uint32_t (&r)[kEpt],
                                                    uint32_t &i0, uint64_t pol) {
-  static_assert(kEpt == 8, "a group is two 4-element vectors");
+  static_assert(kEpt == 8, "a group is one 8-element vector or two 4-element vectors");
   i0 = max(g, c0);
   const uint32_t i1 = min(g + kEpt, c1);
   if (i0 >= i1) return 0u;
   const uint32_t cnt = i1 - i0;
-  if (VEC && cnt == kEpt) {  // i0 == g, a multiple of 8: 16-byte aligned for 4-byte types
+  if (VEC == 2 && cnt == kEpt) {  // i0 == g, a multiple of 8: 32-byte aligned
+    T v[8];
+    uint32_t k[8];
+    ld_stream8(vals + i0, v, pol);
+    ld_stream8(cols + i0, k, pol);
+    ld_stream8(rows + i0, r, pol);
+    T xv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xv[j] = xs(k[j]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) p[j] = mul_rn(v[j], xv[j]);
+  } else if (VEC == 1 && cnt == kEpt) {  // 16-byte aligned: two loads per array
     T v0[4], v1[4];
     uint32_t k0[4], k1[4], q0[4], q1[4];
     ld_stream4(vals + i0, v0, pol);
@@ -1038,7 +1049,7 @@ constexpr uint32_t kNoRow = 0xffffffffu;
 // ---------------------------------------------------------------------------
 // COO in two passes (the default COO and hybrid-tail path).
 // Pass 1, coo_warp_kernel: warp w reduces the 256 elements [256 w, 256 w + 256):
-// lane l loads elements 8 l .. 8 l + 7 (16-byte loads) and sums its runs of
+// lane l loads elements 8 l .. 8 l + 7 (32-byte loads) and sums its runs of
 // equal rows in order; a segmented scan over the lanes (shuffles) carries the
 // runs that cross lanes.  Rows that start and end inside the warp tile are
 // written to y; the tile's head row (continuing from the previous tile) and
@@ -1166,7 +1177,7 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint3
   }
 }
 
-template <typename T, bool VEC, bool ACCUM>
+template <typename T, int VEC, bool ACCUM>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
@@ -1198,13 +1209,23 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
 // warp share the rows' elements (8 each) and combine them with the segmented
 // shuffle scan, whatever the rows' lengths.
 // ---------------------------------------------------------------------------
-template <typename T, bool VEC>
+template <typename T, int VEC>
 __device__ __forceinline__ uint32_t load_product_group(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                                                        const T *__restrict__ x, uint32_t g, uint32_t c1,
                                                        T (&p)[kEpt], uint64_t pol) {
   if (g >= c1) return 0u;
   const uint32_t cnt = min(kEpt, c1 - g);
-  if (VEC && cnt == kEpt) {  // g a multiple of 8: 16-byte aligned for 4-byte types
+  if (VEC == 2 && cnt == kEpt) {  // g a multiple of 8: 32-byte aligned
+    T v[8];
+    uint32_t k[8];
+    ld_stream8(vals + g, v, pol);
+    ld_stream8(cols + g, k, pol);
+    T xv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xv[j] = ld_x(x + k[j]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) p[j] = mul_rn(v[j], xv[j]);
+  } else if (VEC == 1 && cnt == kEpt) {  // 16-byte aligned: two loads per array
     T v0[4], v1[4];
     uint32_t k0[4], k1[4];
     ld_stream4(vals + g, v0, pol);
@@ -1232,7 +1253,7 @@ __device__ __forceinline__ uint32_t load_product_group(const T *__restrict__ val
 
 constexpr uint32_t kTileCnt = kWarpTile + 4;  // per-warp start counts: positions 0..256, padded to 16 bytes
 
-template <typename T, bool VEC>
+template <typename T, int VEC>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     csr_tile_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ tile_prev,
@@ -1395,7 +1416,7 @@ struct scoo_smem_static {
   seg_scan_smem<T> scan;
 };
 
-template <typename T, bool VEC, bool XWIN>
+template <typename T, int VEC, bool XWIN>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : MFP_COO_MINBLOCKS64) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,

@@ -328,6 +328,48 @@ def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
     assert err.value == 0
 
 
+@pytest.mark.parametrize("fmt", ["coo", "csr_vector"])
+def test_warp_tile_load_widths_agree(oracle_lib, fmt):
+    """The warp-tile kernels (COO warp pass, warp-tile CSR) read a lane's 8
+    elements as one 32-byte load per array (32-byte-aligned arrays), as two
+    16-byte loads (16-byte-aligned) or one by one (4-byte-aligned); the three
+    give the same bits."""
+    m = syn("power_law_300k").astype(np.float32)
+    x = synth.vector(9, m.cols).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    coo = F.coo_matrix_class(m)
+    outs = []
+    for off in (0, 16, 4):  # bytes past a 256-byte-aligned allocation
+        keep = []
+
+        def dev(a):
+            raw = torch.zeros(a.nbytes + off, dtype=torch.uint8, device="cuda")
+            raw[off:].copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).ravel()))
+            keep.append(raw)
+            return C.c_void_p(raw.data_ptr() + off)
+        yt = torch.full((m.rows,), float("nan"), device="cuda")
+        if fmt == "coo":
+            nbytes = C.c_size_t()
+            call("mfp_coo_workspace_bytes", m.rows, m.nnz, C.byref(nbytes))
+            ws = torch.zeros(nbytes.value, dtype=torch.uint8, device="cuda")
+            call("mfp_coo_spmv_f32", m.rows, m.cols, m.nnz, dev(coo.data), dev(coo.cols_.view(np.int32)),
+                 dev(coo.rows_.view(np.int32)), C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()),
+                 C.c_void_p(ws.data_ptr()), nbytes.value, stream)
+        else:
+            plan = C.c_void_p()
+            call("mfp_csr_plan_create", m.rows, m.cols, m.nnz, F.ptr(m.row_ptr), 1, None, C.byref(plan))
+            call("mfp_csr_spmv_f32", plan, dev(m.data), dev(m.columns.view(np.int32)), dev(m.row_ptr.view(np.int32)),
+                 C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()), stream)
+            torch.cuda.synchronize()
+            call("mfp_csr_plan_destroy", plan)
+        torch.cuda.synchronize()
+        outs.append(yt.cpu().numpy())
+    for y in outs[1:]:
+        assert np.array_equal(outs[0].view(np.uint32), y.view(np.uint32))
+    check_tol(oracle_lib, m, x, outs[0], f"{fmt} load widths")
+
+
 @pytest.mark.parametrize("fmt", [CSR_ADAPTIVE, COO, HYBRID])
 def test_host_buffer_call_equals_device_call(fmt):
     m = syn("stencil_40").astype(np.float32)
