@@ -20,8 +20,10 @@
  *  - Index arrays are uint32 (the reference uses unsigned int,
  *    common/matrix_converter.h:36-38).  Value arrays are float (f32) or
  *    double (f64), as the reference instantiates (gpu_matrix_multiplier.cu:1219-1302).
- *  - Device arrays passed to the SpMV entry points should start on a 16-byte
- *    boundary (cudaMalloc gives 256); unaligned arrays take a slower path.
+ *  - Device arrays passed to the SpMV entry points should start on a 32-byte
+ *    boundary (cudaMalloc gives 256): kernels that read a whole 32-byte sector
+ *    per thread use one 256-bit load there, two 16-byte loads on 16-byte
+ *    boundaries, and unaligned arrays take a slower path.
  */
 #ifndef MFP_SPMV_H
 #define MFP_SPMV_H
@@ -299,8 +301,9 @@ int mfp_workspace_error(const void *workspace, uint32_t *error);
  * L1-cached read-only path, 1 L2 only (ld.global.cg), 2 read-only without L1
  * allocation.  One partial sum per CTA goes to `out` (at least 148 * 8 =
  * 1184 floats on a B200; fewer -> MFP_ERROR_INVALID_VALUE).  Arrays must be
- * 16-byte aligned.  Its time on a matrix bounds every format's kernel time
- * on that matrix from below. */
+ * 16-byte aligned (32-byte aligned arrays read each thread's sector with one
+ * load, as the formats' kernels do).  Its time on a matrix bounds every
+ * format's kernel time on that matrix from below. */
 int mfp_probe_spmv_loads(int mode, int x_path, uint32_t nnz, const float *values, const uint32_t *col_ids,
                          const float *x, float *out, size_t out_len, void *stream);
 /* The same probe with the x gathers done by TMA (cp.async.bulk.tensor

@@ -33,7 +33,16 @@ __device__ __forceinline__ void ld_stream4(const float *p, float (&v)[4], uint64
                : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
                : "l"(p), "l"(pol));
 }
+// Four doubles are one 32-byte sector when p is 32-byte aligned: one 256-bit
+// load then (two 16-byte loads of one sector would ask L2 for it twice),
+// else two 16-byte loads.  Callers' alignment is uniform over a warp.
 __device__ __forceinline__ void ld_stream4(const double *p, double (&v)[4], uint64_t pol) {
+  if ((reinterpret_cast<uintptr_t>(p) & 31u) == 0) {
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f64 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+                 : "l"(p), "l"(pol));
+    return;
+  }
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
                : "=d"(v[0]), "=d"(v[1])
                : "l"(p), "l"(pol));
@@ -66,6 +75,31 @@ __device__ __forceinline__ void ld_stream8(const uint32_t *p, uint32_t (&v)[8], 
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                : "l"(p), "l"(pol));
+}
+// 32-byte store (p 32-byte aligned).
+__device__ __forceinline__ void st_global8(float *p, const float (&v)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+               "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+
+// 8 consecutive 4-byte words (p 16-byte aligned): one 32-byte load when p is
+// 32-byte aligned, else two 16-byte loads.
+template <typename W>
+__device__ __forceinline__ void ld_stream8_any(const W *p, W (&v)[8], uint64_t pol) {
+  static_assert(sizeof(W) == 4, "4-byte words");
+  if ((reinterpret_cast<uintptr_t>(p) & 31u) == 0) {
+    ld_stream8(p, v, pol);
+    return;
+  }
+  W a[4], b[4];
+  ld_stream4(p, a, pol);
+  ld_stream4(p + 4, b, pol);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = a[k];
+    v[4 + k] = b[k];
+  }
 }
 __device__ __forceinline__ float ld_stream1(const float *p, uint64_t pol) {
   float v;

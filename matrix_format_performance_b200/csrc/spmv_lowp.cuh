@@ -104,14 +104,7 @@ struct lowp_group {
         c[2 * k + 1] = cb + (d[k] >> 16);
       }
     } else {
-      uint32_t c0[4], c1[4];
-      ld_stream4(A.cols + e0, c0, pol);
-      ld_stream4(A.cols + e0 + 4, c1, pol);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        c[k] = c0[k];
-        c[4 + k] = c1[k];
-      }
+      ld_stream8_any(A.cols + e0, c, pol);
     }
   }
   __device__ __forceinline__ void products(const lowp_args<VT, D16> &A, float *dst, uint32_t i) const {
@@ -637,14 +630,7 @@ __global__ void __launch_bounds__(kBlock, D16 && VEC ? MFP_LOWP_ELL_MINBLOCKS : 
                 c[0] <= A.n_cols - 12u;  // (c[0] & ~3) + 12 <= n_cols, overflow-free
         }
       } else {
-        uint32_t c0[4], c1[4];
-        ld_stream4(A.cols + o, c0, pol);
-        ld_stream4(A.cols + o + 4, c1, pol);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          c[j] = c0[j];
-          c[4 + j] = c1[j];
-        }
+        ld_stream8_any(A.cols + o, c, pol);
       }
       float xv[8];
       if (run) {
@@ -660,7 +646,14 @@ __global__ void __launch_bounds__(kBlock, D16 && VEC ? MFP_LOWP_ELL_MINBLOCKS : 
         acc[2 * j + 1] = __fmaf_rn(f.y, xv[2 * j + 1], acc[2 * j + 1]);
       }
     }
-    if (XRUN) {  // 16-byte-aligned y and scale: r is a multiple of 8
+    if (XRUN && ((reinterpret_cast<uintptr_t>(A.y) | reinterpret_cast<uintptr_t>(A.scale)) & 31u) == 0) {
+      // 32-byte-aligned y and scale (r is a multiple of 8): one sector each
+      float sc[8];
+      ld_stream8(A.scale + r, sc, pol);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] *= sc[j];
+      st_global8(A.y + r, acc);
+    } else if (XRUN) {  // 16-byte-aligned y and scale
       const float4 s0 = __ldg(reinterpret_cast<const float4 *>(A.scale + r));
       const float4 s1 = __ldg(reinterpret_cast<const float4 *>(A.scale + r + 4));
       *reinterpret_cast<float4 *>(A.y + r) = make_float4(acc[0] * s0.x, acc[1] * s0.y, acc[2] * s0.z, acc[3] * s0.w);

@@ -2,7 +2,8 @@
 //
 // It issues the memory operations of an SpMV over nnz (value, column) pairs
 // and nothing else: no rows, no reduction by row, one partial sum per CTA.
-//   mode 0  stream the values and column ids (16-byte loads), no x gathers
+//   mode 0  stream the values and column ids (a 32-byte load per array and
+//           thread, on 32-byte-aligned arrays), no x gathers
 //   mode 1  stream the column ids and gather x[col]
 //   mode 2  stream both arrays and gather x[col] (the loads of any format
 //           that reads each nonzero and its x entry once)
@@ -26,7 +27,7 @@ namespace mfp {
 namespace dev {
 
 constexpr int kProbeBlock = 256;
-constexpr int kProbeEpt = 8;  // elements per thread per step: two 16-byte loads per array
+constexpr int kProbeEpt = 8;  // elements per thread per step: one 32-byte sector per array
 
 template <int XPATH>
 __device__ __forceinline__ float probe_x(const float *p) {
@@ -54,26 +55,8 @@ __global__ void __launch_bounds__(kProbeBlock) probe_loads_kernel(uint32_t nnz, 
     const uint32_t e = g * kProbeEpt;
     float v[8];
     uint32_t c[8];
-    if (MODE == 0 || MODE == 2) {
-      float a[4], b[4];
-      ld_stream4(vals + e, a, pol);
-      ld_stream4(vals + e + 4, b, pol);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        v[k] = a[k];
-        v[k + 4] = b[k];
-      }
-    }
-    {
-      uint32_t a[4], b[4];
-      ld_stream4(cols + e, a, pol);
-      ld_stream4(cols + e + 4, b, pol);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        c[k] = a[k];
-        c[k + 4] = b[k];
-      }
-    }
+    if (MODE == 0 || MODE == 2) ld_stream8_any(vals + e, v, pol);
+    ld_stream8_any(cols + e, c, pol);
     if (MODE == 3) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) c[k] &= 4095u;
@@ -156,16 +139,7 @@ __global__ void __launch_bounds__(kG4Warps * 32) probe_gather4_kernel(uint32_t n
   for (uint32_t st = blockIdx.x * kG4Warps + warp; st < steps; st += gridDim.x * kG4Warps) {
     const uint32_t e = st * 256u + lane * 8u;
     uint32_t c[8];
-    {
-      uint32_t a[4], b[4];
-      ld_stream4(cols + e, a, pol);
-      ld_stream4(cols + e + 4, b, pol);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        c[k] = a[k];
-        c[k + 4] = b[k];
-      }
-    }
+    ld_stream8_any(cols + e, c, pol);
     if (lane == 0) mbar_arrive_expect_tx(&bars[warp], bytes);
     __syncwarp();
     tma_gather4(slot, &map, c[0] >> 2, c[1] >> 2, c[2] >> 2, c[3] >> 2, &bars[warp]);

@@ -241,10 +241,10 @@ def test_lowp_ell_accuracy(oracle_lib, name, vt, index16):
 @pytest.mark.parametrize("name", ["stencil_32", "banded_100k"])
 @pytest.mark.parametrize("vt", [BF16, F16])
 def test_lowp_ell_kernel_variants_agree(oracle_lib, name, vt):
-    """The 16-bit-offset ELL kernel's three variants give the same bits: x, y
-    and scales 16-byte aligned (runs of x, 16-byte y stores), y and scales
-    shifted by 4 bytes (8 rows per thread, scalar stores), and q shifted off
-    16-byte alignment (lane-interleaved rows)."""
+    """The 16-bit-offset ELL kernel's variants give the same bits: x, y and
+    scales 32- or 16-byte aligned (runs of x; 32- or 16-byte y stores), y and
+    scales shifted by 4 bytes (8 rows per thread, scalar stores), and q
+    shifted off 16-byte alignment (lane-interleaved rows)."""
     import torch
     m = case(name)
     assert m.rows % 8 == 0
@@ -258,7 +258,7 @@ def test_lowp_ell_kernel_variants_agree(oracle_lib, name, vt):
         return C.c_void_p(p)
 
     outs = []
-    for q_off, ys_off in ((0, 0), (0, 4), (2, 4)):
+    for q_off, ys_off in ((0, 0), (0, 16), (0, 4), (2, 4)):
         qd, od = dev(q, q_off), dev(idx, q_off)
         scd, xd = dev(sc, ys_off), dev(x, 0)
         yraw, yp = _dev_copy(np.full(m.rows, np.nan, np.float32), ys_off)

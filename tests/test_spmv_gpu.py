@@ -328,19 +328,21 @@ def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
     assert err.value == 0
 
 
-@pytest.mark.parametrize("fmt", ["coo", "csr_vector"])
-def test_warp_tile_load_widths_agree(oracle_lib, fmt):
-    """The warp-tile kernels (COO warp pass, warp-tile CSR) read a lane's 8
-    elements as one 32-byte load per array (32-byte-aligned arrays), as two
-    16-byte loads (16-byte-aligned) or one by one (4-byte-aligned); the three
-    give the same bits."""
-    m = syn("power_law_300k").astype(np.float32)
-    x = synth.vector(9, m.cols).astype(np.float32)
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("fmt", ["coo", "csr0", "csr1", "csr2", "ell"])
+def test_load_widths_agree(oracle_lib, fmt, dtype):
+    """Kernels read a thread's 32-byte sector with one 256-bit load on
+    32-byte-aligned arrays, with 16-byte loads on 16-byte-aligned arrays and
+    element by element otherwise; the three give the same bits (COO warp
+    pass, CSR scalar / vector (warp tiles), ELL; FP32 and FP64).  CSR-Adaptive
+    gives the same bits for both vector widths."""
+    m = syn("stencil_40" if fmt == "ell" else "power_law_300k").astype(dtype)
+    x = synth.vector(9, m.cols).astype(dtype)
     xt = torch.from_numpy(x).cuda()
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    coo = F.coo_matrix_class(m)
+    sfx = "f32" if dtype == np.float32 else "f64"
     outs = []
-    for off in (0, 16, 4):  # bytes past a 256-byte-aligned allocation
+    for off in (0, 16, np.dtype(dtype).itemsize):  # bytes past a 256-byte-aligned allocation
         keep = []
 
         def dev(a):
@@ -348,26 +350,35 @@ def test_warp_tile_load_widths_agree(oracle_lib, fmt):
             raw[off:].copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).ravel()))
             keep.append(raw)
             return C.c_void_p(raw.data_ptr() + off)
-        yt = torch.full((m.rows,), float("nan"), device="cuda")
+        yraw = torch.zeros(m.rows * x.itemsize + off, dtype=torch.uint8, device="cuda")
+        yp = C.c_void_p(yraw.data_ptr() + off)
         if fmt == "coo":
+            coo = F.coo_matrix_class(m)
             nbytes = C.c_size_t()
             call("mfp_coo_workspace_bytes", m.rows, m.nnz, C.byref(nbytes))
             ws = torch.zeros(nbytes.value, dtype=torch.uint8, device="cuda")
-            call("mfp_coo_spmv_f32", m.rows, m.cols, m.nnz, dev(coo.data), dev(coo.cols_.view(np.int32)),
-                 dev(coo.rows_.view(np.int32)), C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()),
-                 C.c_void_p(ws.data_ptr()), nbytes.value, stream)
+            call(f"mfp_coo_spmv_{sfx}", m.rows, m.cols, m.nnz, dev(coo.data), dev(coo.cols_.view(np.int32)),
+                 dev(coo.rows_.view(np.int32)), C.c_void_p(xt.data_ptr()), yp, C.c_void_p(ws.data_ptr()),
+                 nbytes.value, stream)
+        elif fmt == "ell":
+            e = F.ell_matrix_class(m)
+            call(f"mfp_ell_spmv_{sfx}", m.rows, m.cols, e.elements_in_rows, dev(e.data), dev(e.columns.view(np.int32)),
+                 C.c_void_p(xt.data_ptr()), yp, stream)
         else:
             plan = C.c_void_p()
-            call("mfp_csr_plan_create", m.rows, m.cols, m.nnz, F.ptr(m.row_ptr), 1, None, C.byref(plan))
-            call("mfp_csr_spmv_f32", plan, dev(m.data), dev(m.columns.view(np.int32)), dev(m.row_ptr.view(np.int32)),
-                 C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()), stream)
+            call("mfp_csr_plan_create", m.rows, m.cols, m.nnz, F.ptr(m.row_ptr), int(fmt[3]), None, C.byref(plan))
+            call(f"mfp_csr_spmv_{sfx}", plan, dev(m.data), dev(m.columns.view(np.int32)),
+                 dev(m.row_ptr.view(np.int32)), C.c_void_p(xt.data_ptr()), yp, stream)
             torch.cuda.synchronize()
             call("mfp_csr_plan_destroy", plan)
         torch.cuda.synchronize()
-        outs.append(yt.cpu().numpy())
-    for y in outs[1:]:
-        assert np.array_equal(outs[0].view(np.uint32), y.view(np.uint32))
-    check_tol(oracle_lib, m, x, outs[0], f"{fmt} load widths")
+        outs.append(yraw[off:].cpu().numpy().view(dtype).copy())
+    assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
+    if fmt == "csr2":  # a whole-CTA row shares its elements among threads differently element by element
+        check_tol(oracle_lib, m, x, outs[2], f"{fmt} {sfx} unaligned")
+    else:
+        assert np.array_equal(outs[0].view(np.uint8), outs[2].view(np.uint8))
+    check_tol(oracle_lib, m, x, outs[0], f"{fmt} {sfx} load widths")
 
 
 @pytest.mark.parametrize("fmt", [CSR_ADAPTIVE, COO, HYBRID])
