@@ -15,8 +15,12 @@ such matrices.
 value    algorithmic bytes of all SpMVs / max-over-ranks device time of the
          kernels (CUDA events on the launching stream; L2 flushed before every
          launch).  Bytes per SpMV: nnz*(4+4) + (rows+1)*4 + cols*4 + rows*4.
-e2e      the same bytes / time of mfp_matrix_spmv_host (host x in, host y
-         out, page-locked buffers, copies inside the timed region).
+e2e      the same bytes / time through the host-buffer API: every step copies
+         its x in from page-locked host memory and its y out, inside the
+         timed region.  value: mfp_matrix_spmv_host_batch over the steps of
+         a format (step i+1's copy-in and step i-1's copy-out overlap step
+         i's kernel); single_call_value: one mfp_matrix_spmv_host per step
+         (copy in, kernel, copy out, wait).
 Multi-GPU (one rank per GPU): --scaling strong (default) splits the one
 power-law matrix into contiguous row blocks balanced by nonzeros
 (partition.rank_shard), x replicated, each rank's y slice its own; value
@@ -474,35 +478,49 @@ def run_engine(args):
     kernel_ms = sum(sum(v) for v in per_fmt_ms.values())
     bracket_ms = wall0.elapsed_time(wall1)
 
-    # e2e: host x in, host y out, through mfp_matrix_spmv_host
+    # e2e: host x in, host y out, through the host-buffer API (page-locked
+    # vectors; one x copied in and one y copied out per step)
+    e_steps = max(1, args.steps)
     hx = torch.from_numpy(x).pin_memory().numpy()
-    hy = torch.empty(m.rows, dtype=torch.float32).pin_memory().numpy()
-    for f in formats:
-        mats[f].spmv_host(hx, hy, stream)
-    e_steps = max(1, min(args.steps, 5))
+    hys = [torch.empty(m.rows, dtype=torch.float32).pin_memory().numpy() for _ in range(e_steps)]
+    for f in formats:  # warm-up; the first pipelined call makes the handle's copy streams
+        mats[f].spmv_host(hx, hys[0], stream)
+        mats[f].spmv_host_batch([hx] * 2, hys[:1] * 2, stream)
     torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e_steps):
+
+    def timed(fn):
+        if ws > 1:
+            dist.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    def pipelined():
         for f in formats:
-            mats[f].spmv_host(hx, hy, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+            mats[f].spmv_host_batch([hx] * e_steps, hys, stream)
+
+    def single_calls():
+        for k in range(e_steps):
+            for f in formats:
+                mats[f].spmv_host(hx, hys[k], stream)
+    e2e_ms = timed(pipelined)
+    e2e_single_ms = timed(single_calls)
 
     # max over ranks; weak scaling sums the ranks' own bytes
-    tt = torch.tensor([kernel_ms, bracket_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    tt = torch.tensor([kernel_ms, bracket_ms, e2e_ms, e2e_single_ms], dtype=torch.float64, device="cuda")
     nb = torch.tensor([float(nbytes_rank)], dtype=torch.float64, device="cuda")
     if ws > 1:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         dist.all_reduce(nb, op=dist.ReduceOp.SUM)
-    kernel_ms, bracket_ms, e2e_ms = tt.tolist()
+    kernel_ms, bracket_ms, e2e_ms, e2e_single_ms = tt.tolist()
     job_bytes = nbytes_global if args.scaling == "strong" else int(nb.item())
     value = job_bytes * len(formats) * args.steps / (kernel_ms * 1e-3) / 1e9
     e2e_value = job_bytes * len(formats) * e_steps / (e2e_ms * 1e-3) / 1e9
+    e2e_single_value = job_bytes * len(formats) * e_steps / (e2e_single_ms * 1e-3) / 1e9
     launch_counts = {f: mats[f].info().kernel_launches for f in formats}
     for f in formats:
         mats[f].close()
@@ -534,7 +552,10 @@ def run_engine(args):
                "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
                        "h2d_bytes_per_step": int(m.cols * 4 * len(formats) * ws),
                        "d2h_bytes_per_step": int(glob[0] * 4 * len(formats)) if args.scaling == "strong"
-                       else int(m.rows * 4 * len(formats) * ws), "steps": e_steps},
+                       else int(m.rows * 4 * len(formats) * ws), "steps": e_steps,
+                       "mode": "mfp_matrix_spmv_host_batch per format over the steps: a step's copies overlap "
+                               "the neighbouring steps' kernels",
+                       "single_call_value": round(e2e_single_value, 1)},
                "gpu_launches": args.steps * sum(launch_counts[f] for f in formats),
                "clocks": clocks}
         if ws == 1 and not args.no_extras:

@@ -596,6 +596,15 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream);
  * with lanes per row, ELL, SCOO, the reduced-precision layouts), the kernel
  * stores y straight into host_y, so the copy-out overlaps the kernel. */
 int mfp_matrix_spmv_host(mfp_matrix *m, const void *host_x, void *host_y, void *stream);
+/* count independent products host_y[i] = A*host_x[i] with HOST vectors,
+ * pipelined: x_{i+1} is copied in while SpMV i runs and y_{i-1} is copied
+ * out (two device staging pairs, two copy streams of the handle, made on
+ * the first call).  The kernels run in order on `stream`; the call returns
+ * when every y is in host memory.  Page-locked host vectors give the copies
+ * full PCIe bandwidth and let them overlap.  Engine extension: the serving
+ * form of mfp_matrix_spmv_host. */
+int mfp_matrix_spmv_host_batch(mfp_matrix *m, uint32_t count, const void *const *host_x, void *const *host_y,
+                               void *stream);
 
 /* ------------------------------------------------------------------------- */
 /* Measurement records — measurement_class (common/measurement_class.h:11-58) */

@@ -121,6 +121,7 @@ _PROTOS = {
     "mfp_matrix_get_info": [vp, C.POINTER(MatrixInfo)],
     "mfp_matrix_spmv": [vp, vp, vp, vp],
     "mfp_matrix_spmv_host": [vp, vp, vp, vp],
+    "mfp_matrix_spmv_host_batch": [vp, u32, vp, vp, vp],
     "mfp_measurement_make": [C.c_char_p, f64, f64, f64, C.POINTER(Measurement)],
     "mfp_compare_results_f32": [u32, vp, vp, C.POINTER(f64), P_u32],
     "mfp_compare_results_f64": [u32, vp, vp, C.POINTER(f64), P_u32],

@@ -1160,6 +1160,11 @@ struct mfp_matrix {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   void *dx = nullptr, *dy = nullptr;  // staging for the host-buffer call
+  // second staging pair, copy streams and events of the pipelined host-buffer
+  // call (made on its first use)
+  void *dx2 = nullptr, *dy2 = nullptr;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_in[2] = {}, ev_k[2] = {}, ev_out[2] = {};
   int lowp_vt = 0;                    // reduced-precision CSR: MFP_BF16 / MFP_F16
   float *scale = nullptr;
   uint16_t *delta = nullptr;          // 16-bit column deltas (else cols_a)
@@ -1254,6 +1259,12 @@ extern "C" {
 
 int mfp_matrix_destroy(mfp_matrix *m) {
   if (!m) return ok();
+  if (m->s_in) cudaStreamSynchronize(m->s_in);
+  if (m->s_out) cudaStreamSynchronize(m->s_out);
+  for (cudaEvent_t e : {m->ev_start, m->ev_in[0], m->ev_in[1], m->ev_k[0], m->ev_k[1], m->ev_out[0], m->ev_out[1]})
+    if (e) cudaEventDestroy(e);
+  if (m->s_in) cudaStreamDestroy(m->s_in);
+  if (m->s_out) cudaStreamDestroy(m->s_out);
   for (void *p : m->allocs) cudaFree(p);
   mfp_csr_plan_destroy(m->plan);
   delete m;
@@ -1787,6 +1798,62 @@ int mfp_matrix_spmv_host(mfp_matrix *m, const void *hx, void *hy, void *stream) 
   if (st) return st;
   if (m->rows && !y_mapped)
     CUDA_TRY(cudaMemcpyAsync(hy, m->dy, (size_t)m->rows * vs, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync y");
+  CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return ok();
+}
+
+int mfp_matrix_spmv_host_batch(mfp_matrix *m, uint32_t count, const void *const *hx, void *const *hy,
+                               void *stream) {
+  if (!m || (count && (!hx || !hy))) return fail(MFP_ERROR_INVALID_VALUE, "null argument");
+  for (uint32_t i = 0; i < count; ++i)
+    if (!hy[i] || (!hx[i] && m->cols)) return fail(MFP_ERROR_INVALID_VALUE, "null host vector %u", i);
+  if (count == 0) return ok();
+  const size_t vs = value_size(m->value_type);
+  cudaStream_t s = as_stream(stream);
+  if (!m->s_in) {
+    unsigned char *a = nullptr, *b = nullptr;
+    int st = track(m, &a, (size_t)std::max(1u, m->cols) * vs);
+    if (!st) st = track(m, &b, (size_t)std::max(1u, m->rows) * vs);
+    if (st) return st;
+    m->dx2 = a;
+    m->dy2 = b;
+    for (cudaEvent_t *e : {&m->ev_start, &m->ev_in[0], &m->ev_in[1], &m->ev_k[0], &m->ev_k[1], &m->ev_out[0],
+                           &m->ev_out[1]})
+      CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreateWithFlags");
+    CUDA_TRY(cudaStreamCreateWithFlags(&m->s_out, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    CUDA_TRY(cudaStreamCreateWithFlags(&m->s_in, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+  }
+  void *dx[2] = {m->dx, m->dx2}, *dy[2] = {m->dy, m->dy2};
+  // the copies start after the work already on `stream`
+  CUDA_TRY(cudaEventRecord(m->ev_start, s), "cudaEventRecord");
+  CUDA_TRY(cudaStreamWaitEvent(m->s_in, m->ev_start, 0), "cudaStreamWaitEvent");
+  CUDA_TRY(cudaStreamWaitEvent(m->s_out, m->ev_start, 0), "cudaStreamWaitEvent");
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint32_t b = i & 1u;
+    // x_i into staging b once SpMV i - 2 has read it
+    if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(m->s_in, m->ev_k[b], 0), "cudaStreamWaitEvent");
+    if (m->cols)
+      CUDA_TRY(cudaMemcpyAsync(dx[b], hx[i], (size_t)m->cols * vs, cudaMemcpyHostToDevice, m->s_in),
+               "cudaMemcpyAsync x");
+    CUDA_TRY(cudaEventRecord(m->ev_in[b], m->s_in), "cudaEventRecord");
+    // SpMV i once x_i is in and y_{i-2} is out of staging b
+    CUDA_TRY(cudaStreamWaitEvent(s, m->ev_in[b], 0), "cudaStreamWaitEvent");
+    if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(s, m->ev_out[b], 0), "cudaStreamWaitEvent");
+    const int st = mfp_matrix_spmv(m, dx[b], dy[b], stream);
+    if (st) {
+      cudaStreamSynchronize(m->s_in);
+      cudaStreamSynchronize(m->s_out);
+      return st;
+    }
+    CUDA_TRY(cudaEventRecord(m->ev_k[b], s), "cudaEventRecord");
+    CUDA_TRY(cudaStreamWaitEvent(m->s_out, m->ev_k[b], 0), "cudaStreamWaitEvent");
+    if (m->rows)
+      CUDA_TRY(cudaMemcpyAsync(hy[i], dy[b], (size_t)m->rows * vs, cudaMemcpyDeviceToHost, m->s_out),
+               "cudaMemcpyAsync y");
+    CUDA_TRY(cudaEventRecord(m->ev_out[b], m->s_out), "cudaEventRecord");
+  }
+  // `stream` ends after the last copy-out (copies are ordered on s_out)
+  CUDA_TRY(cudaStreamWaitEvent(s, m->ev_out[(count - 1u) & 1u], 0), "cudaStreamWaitEvent");
   CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   return ok();
 }

@@ -179,6 +179,17 @@ class DeviceMatrix:
         assert x.dtype == self.dtype and y.dtype == self.dtype
         call("mfp_matrix_spmv_host", self._h, ptr(x), ptr(y), _stream(stream))
 
+    def spmv_host_batch(self, xs: list, ys: list, stream=None) -> None:
+        """ys[i] = A @ xs[i] for host vectors, copies overlapped with the
+        kernels (mfp_matrix_spmv_host_batch); page-locked vectors overlap."""
+        assert len(xs) == len(ys)
+        for x, y in zip(xs, ys):
+            assert x.dtype == self.dtype and y.dtype == self.dtype
+        n = len(xs)
+        px = (C.c_void_p * max(1, n))(*[x.ctypes.data for x in xs])
+        py = (C.c_void_p * max(1, n))(*[y.ctypes.data for y in ys])
+        call("mfp_matrix_spmv_host_batch", self._h, n, px, py, _stream(stream))
+
     def time(self, x, y, reps: int = 20, flush_l2: bool = True, stream=None) -> tuple[float, float]:
         mean, med = C.c_double(), C.c_double()
         call("mfp_matrix_time", self._h, _dptr(x), _dptr(y), reps, int(flush_l2), _stream(stream),

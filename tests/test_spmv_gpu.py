@@ -381,6 +381,34 @@ def test_load_widths_agree(oracle_lib, fmt, dtype):
     check_tol(oracle_lib, m, x, outs[0], f"{fmt} {sfx} load widths")
 
 
+@pytest.mark.parametrize("fmt", [CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE, ELL, COO, SCOO, HYBRID])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_pipelined_host_batch_equals_device_calls(fmt, dtype):
+    """mfp_matrix_spmv_host_batch: 1, 2 and 5 independent host vectors, page
+    locked or not, give the bits of one device call per vector."""
+    m = syn("stencil_40").astype(dtype)
+    dm = DeviceMatrix.build(m, fmt, hybrid_width=20)
+    try:
+        for n, pinned in ((1, True), (2, False), (5, True)):
+            xs = [synth.vector(20 + i, m.cols).astype(dtype) for i in range(n)]
+            if pinned:
+                xs = [torch.from_numpy(x).pin_memory().numpy() for x in xs]
+                ys = [torch.full((m.rows,), float("nan"), dtype=torch.from_numpy(xs[0][:1]).dtype).pin_memory().numpy()
+                      for _ in range(n)]
+            else:
+                ys = [np.full(m.rows, np.nan, dtype) for _ in range(n)]
+            dm.spmv_host_batch(xs, ys)
+            for x, y in zip(xs, ys):
+                xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+                yt = torch.empty(m.rows, dtype=xt.dtype, device="cuda")
+                dm.spmv(xt, yt)
+                torch.cuda.synchronize()
+                assert np.array_equal(y.view(np.uint8), yt.cpu().numpy().view(np.uint8))
+        dm.spmv_host_batch([], [])
+    finally:
+        dm.close()
+
+
 @pytest.mark.parametrize("fmt", [CSR_ADAPTIVE, COO, HYBRID])
 def test_host_buffer_call_equals_device_call(fmt):
     m = syn("stencil_40").astype(np.float32)
