@@ -240,7 +240,7 @@ typedef struct mfp_csr_config {
                                   rows with a segmented shuffle scan; a fix-up launch adds the
                                   rows that cross tiles), else 4 lanes per row */
   uint32_t bin_nnz;            /* CSR-Adaptive elements per row bin; 0 = default */
-  uint32_t piece_nnz;          /* elements per long-row piece; 0 = default (4096) */
+  uint32_t piece_nnz;          /* elements per long-row piece; 0 = default (65536) */
   uint32_t assist_threshold;   /* scalar/vector: rows longer than this (and not long) are
                                   reduced by a whole warp; 0 = default (64);
                                   UINT32_MAX = never (keeps the reference summation order) */
