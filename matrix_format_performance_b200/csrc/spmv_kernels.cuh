@@ -1074,17 +1074,18 @@ __device__ __forceinline__ void coo_put(T *y, uint32_t n_rows, uint32_t row, T v
   if (row < n_rows) y[row] = ACCUM ? add_rn(y[row], v) : v;
 }
 
-// The reduction of one warp tile [c0, c1) of nnz elements, the lane's cnt
-// products pr and rows rw in hand (rows non-decreasing); prv / nxt are the
-// rows of the elements just before and after the tile (kNoRow at the ends).
+// The reduction of one warp tile ending at c1 (of nnz elements), lane l's
+// group starting at g0 + 8 l, the lane's cnt products pr and rows rw in hand
+// (rows non-decreasing); prv / nxt are the rows of the elements just before
+// and after the tile (kNoRow at the ends).
 template <typename T, bool ACCUM>
-__device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t c0, uint32_t c1, uint32_t nnz,
+__device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t g0, uint32_t c1, uint32_t nnz,
                                                  uint32_t n_rows, const T (&pr)[kEpt], const uint32_t (&rw)[kEpt],
                                                  uint32_t cnt, uint32_t prv, uint32_t nxt, T *__restrict__ y,
                                                  const coo_carry<T> &cw, coo_ws_header *hdr) {
   const uint32_t lane = threadIdx.x & 31u;
   const bool active = cnt > 0;
-  const uint32_t last_lane = (c1 - c0 - 1u) / kEpt;
+  const uint32_t last_lane = (c1 - g0 - 1u) / kEpt;
   // runs inside the lane: the first and last run's sums; middle runs are whole rows
   uint32_t rf = kNoRow, rl = kNoRow;
   T sf = T(0), sl = T(0);
@@ -1411,9 +1412,18 @@ __global__ void __launch_bounds__(kBlock) coo_fixup_kernel(uint32_t n_tiles, uin
 // SCOO: one CTA per slice; row accumulators and (optionally) the slice's x
 // window live in dynamic shared memory.
 // ---------------------------------------------------------------------------
+// SCOO in warp tiles: a slice of up to kScooTiles tiles (131,072 elements)
+// keeps its tiles' carries in shared memory.
+constexpr uint32_t kScooTiles = 512;
 template <typename T>
 struct scoo_smem_static {
-  seg_scan_smem<T> scan;
+  union {
+    seg_scan_smem<T> scan;
+    struct {
+      T head[kScooTiles], tail[kScooTiles];
+      uint32_t flags[kScooTiles], tail_row[kScooTiles];
+    } t;
+  };
 };
 
 template <typename T, int VEC, bool XWIN>
@@ -1450,6 +1460,55 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
     }
   }
   __syncthreads();
+  {
+    // Warp tiles: warp w reduces the slice's 256-element tiles w, w + 8, ...
+    // with the COO warp-tile reduction, rows that start and end in a tile
+    // going straight into the accumulator; after one barrier, each row that
+    // crosses tiles is summed in tile order from the tiles' carries.  No
+    // barrier per chunk; the same bits on every run.
+    const uint32_t base8 = eb & ~7u;
+    const uint32_t n_tiles = eb < ee ? (ee - base8 + kWarpTile - 1u) / kWarpTile : 0u;
+    if (n_tiles <= kScooTiles) {
+      const uint32_t lane = threadIdx.x & 31u;
+      coo_carry<T> cw;
+      cw.head = sm.t.head;
+      cw.tail = sm.t.tail;
+      cw.flags = sm.t.flags;
+      cw.tail_row = sm.t.tail_row;
+      T *yrow = acc - row0;  // yrow[r] = acc[r - row0] for the slice's rows
+      for (uint32_t t = threadIdx.x >> 5; t < n_tiles; t += kBlock / 32u) {
+        const uint32_t g0 = base8 + t * kWarpTile;
+        const uint32_t c0 = max(eb, g0), c1 = min(ee, g0 + kWarpTile);
+        T pr[kEpt];
+        uint32_t rw[kEpt], i0 = 0;
+        const uint32_t g = g0 + lane * kEpt;
+        const uint32_t cnt =
+            (XWIN && use_win) ? load_run_group<T, VEC>(vals, cidx, ridx, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
+                              : load_run_group<T, VEC>(vals, cidx, ridx, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
+        const uint32_t prv = c0 > eb ? __ldg(ridx + c0 - 1u) : kNoRow;
+        const uint32_t nxt = c1 < ee ? __ldg(ridx + c1) : kNoRow;
+        warp_tile_reduce<T, true>(t, g0, c1, ee, row0 + nrows, pr, rw, cnt, prv, nxt, yrow, cw, nullptr);
+      }
+      __syncthreads();
+      // a row that starts in tile t and goes on: its tail, then the following
+      // tiles' heads in order, up to the tile where it ends
+      for (uint32_t t = threadIdx.x; t < n_tiles; t += kBlock) {
+        const uint32_t f = sm.t.flags[t];
+        if (!(f & kTailCont) || ((f & kOneRow) && (f & kHeadCont))) continue;
+        T sum = sm.t.tail[t];
+        for (uint32_t u = t + 1u; u < n_tiles; ++u) {
+          const uint32_t fu = sm.t.flags[u];
+          sum = add_rn(sum, sm.t.head[u]);
+          if (!((fu & kOneRow) && (fu & kTailCont))) break;
+        }
+        acc[sm.t.tail_row[t] - row0] = sum;
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];
+      return;
+    }
+  }
+  // a slice of more than kScooTiles tiles: whole-CTA chunks of 2048 elements
   auto emit = [&](uint32_t row, T total, bool, bool) {
     const uint32_t lr = row - row0;
     if (lr < nrows) acc[lr] = add_rn(acc[lr], total);

@@ -329,6 +329,31 @@ def test_device_pointer_entry_points_and_unaligned_arrays(oracle_lib):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_scoo_tiles_and_chunk_fallback(oracle_lib, dtype):
+    """SCOO slices reduced in warp tiles (rows crossing tiles summed in tile
+    order), and a slice of more than 512 tiles (a 140,000-element row plus
+    neighbours) that takes the whole-CTA chunk path; empty rows on both
+    sides; the same bits on a second run."""
+    rng = np.random.default_rng(31)
+    rows, cols = 3000, 200_000
+    lens = rng.integers(0, 4, rows)
+    lens[1500] = 140_000          # > 512 tiles of 256 in its slice
+    lens[700] = 130_000 // 2      # ~254 tiles: the tile path with a long carry chain
+    lens[701:705] = 0
+    lens[2990:] = 0
+    rp = np.zeros(rows + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    colv = np.concatenate([np.sort(rng.choice(cols, n, replace=False)) if n else np.zeros(0, np.int64)
+                           for n in lens]).astype(np.uint32)
+    vals = rng.uniform(-1, 1, int(rp[-1]))
+    m = F.csr_matrix_class.from_arrays(rows, cols, rp.astype(np.uint32), colv, vals, dtype)
+    x = synth.vector(5, cols).astype(dtype)
+    a, b = run(m, SCOO, x, reps=2)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    check_tol(oracle_lib, m, x, a, "scoo tiles / chunks")
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("fmt", ["coo", "csr0", "csr1", "csr2", "ell"])
 def test_load_widths_agree(oracle_lib, fmt, dtype):
     """Kernels read a thread's 32-byte sector with one 256-bit load on
