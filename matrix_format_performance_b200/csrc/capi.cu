@@ -183,6 +183,7 @@ struct mfp_csr_plan {
   // each 256-element tile, and the COO-style workspace of the fix-up pass
   uint4 *blk = nullptr;  // per row block: element range and flags (see csr_args::blk)
   bool fast = false;     // row blocks without long rows start their loads before the row_ptr barrier
+  bool binned = false;   // CSR scalar on the CSR-Adaptive bins, one thread per row
   bool tile = false;
   uint32_t *tile_prev = nullptr;
   void *tile_ws = nullptr;
@@ -338,8 +339,17 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
   plan->nnz = nnz;
   if (cfg.piece_nnz == 0) cfg.piece_nnz = kDefaultPiece;
   cfg.piece_nnz = std::max(cfg.piece_nnz, 256u);
-  if (algo == MFP_CSR_ADAPTIVE) {
+  // CSR scalar on short rows (mean length below 16, automatic kernel, not
+  // the exact-order setting): the CSR-Adaptive bins, which balance elements
+  // per CTA, with each row summed by one thread in CSR order.  Measured on
+  // B200 against 256-row blocks, FP32: power-law 4M 0.185 -> 0.162 ms,
+  // 4M rows of 6-9 uniform elements 0.166 -> 0.160 ms.  From mean 16 (the
+  // 27-point stencil, banded 8M) a bin holds too few rows for its threads.
+  const bool exact = cfg.long_row_threshold == UINT32_MAX && cfg.assist_threshold == UINT32_MAX;
+  plan->binned = algo == MFP_CSR_SCALAR && cfg.kernel == 0 && !exact && rows && (double)nnz / rows < 16.0;
+  if (algo == MFP_CSR_ADAPTIVE || plan->binned)
     cfg.bin_nnz = cfg.bin_nnz ? std::min(cfg.bin_nnz, kMaxBin) : kMaxBin;
+  if (algo == MFP_CSR_ADAPTIVE) {
     if (cfg.long_row_threshold == 0) cfg.long_row_threshold = cfg.bin_nnz;
   } else {
     if (cfg.long_row_threshold == 0) cfg.long_row_threshold = kDefaultLong;
@@ -395,7 +405,7 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
     ++nlong;
   }
   std::vector<uint32_t> blocks;
-  if (algo == MFP_CSR_ADAPTIVE) {
+  if (algo == MFP_CSR_ADAPTIVE || plan->binned) {
     blocks.push_back(0);
     uint32_t cur_rows = 0, cur_nnz = 0;
     const uint32_t max_rows = 4 * d::kBlock;
@@ -435,8 +445,9 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
   {
     std::vector<uint64_t> cost(order.size());
     for (uint32_t b = 0; b < plan->n_main; ++b) {
-      const uint32_t r0 = algo == MFP_CSR_ADAPTIVE ? blocks[b] : b * d::kBlock;
-      const uint32_t r1 = algo == MFP_CSR_ADAPTIVE ? blocks[b + 1] : std::min(rows, r0 + d::kBlock);
+      const bool bins = algo == MFP_CSR_ADAPTIVE || plan->binned;
+      const uint32_t r0 = bins ? blocks[b] : b * d::kBlock;
+      const uint32_t r1 = bins ? blocks[b + 1] : std::min(rows, r0 + d::kBlock);
       uint64_t c = r1 - r0;
       for (uint32_t r = r0; r < r1; ++r) {
         const uint32_t len = rp[r + 1] - rp[r];
@@ -625,7 +636,13 @@ int csr_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols, cons
   const bool fast = plan->fast && plan->blk;
   switch (plan->algo) {
     case 0:
-      if (fast) { MFP_CSR_LAUNCH(0, true) } else { MFP_CSR_LAUNCH(0, false) }
+      if (plan->binned) {
+        MFP_CSR_LAUNCH(3, false)
+      } else if (fast) {
+        MFP_CSR_LAUNCH(0, true)
+      } else {
+        MFP_CSR_LAUNCH(0, false)
+      }
       break;
     case 1:
       if (fast) { MFP_CSR_LAUNCH(1, true) } else { MFP_CSR_LAUNCH(1, false) }

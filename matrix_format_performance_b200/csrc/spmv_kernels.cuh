@@ -900,8 +900,10 @@ __device__ __forceinline__ void csr_rowblock_main(const csr_args<T> &A, csr_smem
 // staged whole (the binning caps their elements at bin_nnz <= kChunk - 4) and
 // reduced from shared memory by power-of-two lane groups; a single-row bin is
 // reduced by the whole CTA straight from global memory; a single row above
-// the long threshold belongs to pieces.
-template <typename T, bool VEC>
+// the long threshold belongs to pieces.  SEQ (CSR scalar on short rows): the
+// same bins, each row summed by one thread in CSR order (rows above the
+// assist threshold by a warp).
+template <typename T, bool VEC, bool SEQ = false>
 __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem<T> &sm, uint64_t pol,
                                                   uint32_t blk) {
   const uint32_t rb = A.row_blocks[blk], re = A.row_blocks[blk + 1];
@@ -931,7 +933,7 @@ __device__ __forceinline__ void csr_adaptive_main(const csr_args<T> &A, csr_smem
   // most 227 rows, within the 256-entry list)
   const uint32_t athr = max(A.assist_thr, 8u);
   uint32_t tpr = 1;
-  if (nrows <= (uint32_t)kBlock) {
+  if (!SEQ && nrows <= (uint32_t)kBlock) {
     tpr = kBlock / nrows;  // >= 1
     tpr = tpr >= 32 ? 32u : (1u << (31 - __clz(tpr)));
     const uint32_t grp = t / tpr, lane = t % tpr;
@@ -989,8 +991,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? (ALGO != 1 ? MFP_CSR_
     return;
   }
   const uint32_t b = w;
-  if (ALGO == 2)
-    csr_adaptive_main<T, VEC>(A, sm, pol, b);
+  if (ALGO == 2 || ALGO == 3)
+    csr_adaptive_main<T, VEC, ALGO == 3>(A, sm, pol, b);
   else
     csr_rowblock_main<T, ALGO, VEC, FAST>(A, sm, pol, b);
 }
