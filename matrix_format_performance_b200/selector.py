@@ -6,11 +6,13 @@ pattern (mfp_selector_features):
 - **network**: an ensemble of MLPs 12-64-64-28 (FP32, ReLU), trained from
   different seeds; their 28 outputs, averaged, are the predicted log time,
   relative to the fastest, of the 7 formats x 4 launch configurations of
-  CONFIGS (averaging cuts the variance of single networks: on the measured
-  held-out set one network chose within 5% of the best for 85% of the
-  matrices, ten averaged for 91.5%);
+  CONFIGS (averaging cuts the variance of single networks);
 - **choice**: the selector takes the smallest prediction among the
-  configurations the matrix admits;
+  configurations the matrix admits; with verify=k it times the k smallest
+  on the matrix (k of the 28 configurations) and takes the fastest, which
+  absorbs the network's near-ties (on the measured held-out set: within 5%
+  of the best for 86% of the matrices from the prediction alone, 95% with
+  the three best predictions timed);
 - **training**: on the engine's own kernels (mfp_mlp_forward /
   mfp_mlp_backward / mfp_mlp_adam), against times the engine measured on
   seeded synthetic matrices, with a masked mean-squared error;
@@ -252,23 +254,38 @@ class Selector:
         return (acc / len(self.params)).cpu().numpy()
 
     def choose(self, F: np.ndarray, admissible_mask: np.ndarray) -> np.ndarray:
+        return self.candidates(F, admissible_mask, 1)[:, 0]
+
+    def candidates(self, F: np.ndarray, admissible_mask: np.ndarray, k: int) -> np.ndarray:
+        """The k admissible slots with the smallest predictions, best first,
+        [n, k] (a matrix admitting fewer repeats its last)."""
         pred = self.predict_slots(F)
-        pred = np.where(np.atleast_2d(admissible_mask), pred, np.inf)
-        return pred.argmin(axis=1)
+        mask = np.atleast_2d(admissible_mask)
+        pred = np.where(mask, pred, np.inf)
+        order = np.argsort(pred, axis=1, kind="stable")[:, :k]
+        n_ok = np.maximum(mask.sum(axis=1), 1)
+        return np.where(np.arange(k)[None, :] < n_ok[:, None], order, order[:, [0]])
 
     def in_range(self, f: np.ndarray, margin: float = 0.05) -> bool:
         span = np.maximum(self.hi - self.lo, 1e-6)
         return bool(np.all(f >= self.lo - margin * span) and np.all(f <= self.hi + margin * span))
 
-    def select(self, m: csr_matrix_class, sweep_if_unsure: bool = True, reps: int = 5) -> tuple[int, str]:
-        """(slot, how): the predicted slot, or the exhaustive sweep's best when
-        the matrix lies outside the training range."""
+    def select(self, m: csr_matrix_class, sweep_if_unsure: bool = True, reps: int = 5,
+               verify: int = 1) -> tuple[int, str]:
+        """(slot, how): the predicted slot ("predicted"); with verify=k > 1 the
+        fastest of the k best predictions, timed on the matrix ("verified");
+        the exhaustive sweep's best when the matrix lies outside the training
+        range ("sweep")."""
         f = features(m)
         ok = admissible(m)
         if sweep_if_unsure and not self.in_range(f):
             t = sweep(m, reps=reps)
             return int(np.argmin(t)), "sweep"
-        return int(self.choose(f, ok)[0]), "predicted"
+        cand = self.candidates(f, ok, max(1, verify))[0]
+        if verify <= 1:
+            return int(cand[0]), "predicted"
+        t = sweep(m, reps=reps, slots=sorted(set(int(c) for c in cand)))
+        return int(np.argmin(t)), "verified"
 
     def save(self, path) -> None:
         np.savez(path, params=self.params, mu=self.mu, sigma=self.sigma, lo=self.lo, hi=self.hi,
