@@ -1256,7 +1256,7 @@ __device__ __forceinline__ uint32_t load_product_group(const T *__restrict__ val
 
 constexpr uint32_t kTileCnt = kWarpTile + 4;  // per-warp start counts: positions 0..256, padded to 16 bytes
 
-template <typename T, int VEC>
+template <typename T, int VEC, bool WIDE = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     csr_tile_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ row_ptr, const uint32_t *__restrict__ tile_prev,
@@ -1277,11 +1277,21 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
   // tile, which the last tile does not need
   const uint32_t lim = c1 < nnz ? c1 : c1 - 1u;
   __syncwarp();
-  for (uint32_t j0 = prv + 1u;; j0 += 32u) {  // prv + 1 wraps to 0 for the first tile
-    const uint32_t j = j0 + lane;
-    const uint32_t b = j < n_rows ? __ldg(row_ptr + j) : 0xffffffffu;  // start of row j (>= c0)
-    if (b <= lim) atomicAdd(&sc[b - c0], 1u);
-    if (__any_sync(0xffffffffu, b > lim)) break;
+  // 32 row starts per round trip, or 64 (WIDE) when a tile holds more than
+  // 32 rows on average
+  for (uint32_t j0 = prv + 1u;; j0 += WIDE ? 64u : 32u) {  // prv + 1 wraps to 0 for the first tile
+    const uint32_t ja = j0 + lane;
+    const uint32_t ba = ja < n_rows ? __ldg(row_ptr + ja) : 0xffffffffu;  // start of row ja (>= c0)
+    if (WIDE) {
+      const uint32_t jb = ja + 32u;
+      const uint32_t bb = jb < n_rows ? __ldg(row_ptr + jb) : 0xffffffffu;
+      if (ba <= lim) atomicAdd(&sc[ba - c0], 1u);
+      if (bb <= lim) atomicAdd(&sc[bb - c0], 1u);
+      if (__any_sync(0xffffffffu, bb > lim)) break;  // rows are sorted by start: bb >= ba
+    } else {
+      if (ba <= lim) atomicAdd(&sc[ba - c0], 1u);
+      if (__any_sync(0xffffffffu, ba > lim)) break;
+    }
   }
   __syncwarp();
   // row of each element: prv + the row starts at or before it
