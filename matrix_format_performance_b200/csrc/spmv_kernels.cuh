@@ -1487,7 +1487,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
       cw.tail = sm.t.tail;
       cw.flags = sm.t.flags;
       cw.tail_row = sm.t.tail_row;
-      T *yrow = acc - row0;  // yrow[r] = acc[r - row0] for the slice's rows
+      // rows go in slice-local (r - row0, unsigned): a row id outside the
+      // slice (invalid input) fails the bound checks and is dropped
       for (uint32_t t = threadIdx.x >> 5; t < n_tiles; t += kBlock / 32u) {
         const uint32_t g0 = base8 + t * kWarpTile;
         const uint32_t c0 = max(eb, g0), c1 = min(ee, g0 + kWarpTile);
@@ -1497,9 +1498,11 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
         const uint32_t cnt =
             (XWIN && use_win) ? load_run_group<T, VEC>(vals, cidx, ridx, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
                               : load_run_group<T, VEC>(vals, cidx, ridx, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
-        const uint32_t prv = c0 > eb ? __ldg(ridx + c0 - 1u) : kNoRow;
-        const uint32_t nxt = c1 < ee ? __ldg(ridx + c1) : kNoRow;
-        warp_tile_reduce<T, true>(t, g0, c1, ee, row0 + nrows, pr, rw, cnt, prv, nxt, yrow, cw, nullptr);
+#pragma unroll
+        for (int k = 0; k < kEpt; ++k) rw[k] -= row0;
+        const uint32_t prv = c0 > eb ? __ldg(ridx + c0 - 1u) - row0 : kNoRow;
+        const uint32_t nxt = c1 < ee ? __ldg(ridx + c1) - row0 : kNoRow;
+        warp_tile_reduce<T, true>(t, g0, c1, ee, nrows, pr, rw, cnt, prv, nxt, acc, cw, nullptr);
       }
       __syncthreads();
       // a row that starts in tile t and goes on: its tail, then the following
@@ -1513,7 +1516,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
           sum = add_rn(sum, sm.t.head[u]);
           if (!((fu & kOneRow) && (fu & kTailCont))) break;
         }
-        acc[sm.t.tail_row[t] - row0] = sum;
+        const uint32_t lr = sm.t.tail_row[t];
+        if (lr < nrows) acc[lr] = sum;
       }
       __syncthreads();
       for (uint32_t i = threadIdx.x; i < nrows; i += kBlock) y[row0 + i] = acc[i];

@@ -353,6 +353,44 @@ def test_scoo_tiles_and_chunk_fallback(oracle_lib, dtype):
     check_tol(oracle_lib, m, x, a, "scoo tiles / chunks")
 
 
+def test_raw_scoo_row_ids_outside_their_slice_stay_in_bounds(oracle_lib):
+    """mfp_scoo_spmv_f32 on caller arrays where one element's row id points
+    into the previous slice (inside a long row the warp tiles carry across
+    tiles) and another's beyond the matrix: the slice's shared-memory
+    accumulator is never indexed out of range, every other row keeps the
+    bits of the unchanged arrays, and the two rows get finite values (which
+    the invalid input leaves unspecified)."""
+    m = syn("power_law_300k").astype(np.float32)
+    sc = F.scoo_matrix_class(148, 49152, m)
+    sp = sc.slices_ptr.astype(np.int64)
+    s = int(np.argmax(np.diff(sp)[1:])) + 1            # a slice > 0 with many elements
+    e1, e2 = int(sp[s]) + 300, int(sp[s + 1]) - 1
+    bad = sc.r_index.copy()
+    rows_hit = [int(bad[e1]), int(bad[e2])]
+    assert rows_hit[0] != rows_hit[1]
+    bad[e1] = s * sc.slice_size - 1                       # a row of the previous slice
+    bad[e2] = m.rows + 5                                  # beyond the matrix
+    x = synth.vector(12, m.cols).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    v, ci, sp_d = d(sc.values), d(sc.c_index.view(np.int32)), d(sc.slices_ptr.view(np.int32))
+    outs = []
+    for ri in (sc.r_index, bad):
+        rt = d(ri.view(np.int32))
+        yt = torch.full((m.rows,), float("nan"), device="cuda")
+        call("mfp_scoo_spmv_f32", m.rows, m.cols, sc.slices_count, sc.slice_size, C.c_void_p(v.data_ptr()),
+             C.c_void_p(ci.data_ptr()), C.c_void_p(rt.data_ptr()), C.c_void_p(sp_d.data_ptr()), None, 0, None,
+             C.c_void_p(xt.data_ptr()), C.c_void_p(yt.data_ptr()), None)
+        torch.cuda.synchronize()
+        outs.append(yt.cpu().numpy())
+    good, y = outs
+    check_tol(oracle_lib, m, x, good, "raw scoo")
+    others = np.ones(m.rows, bool)
+    others[rows_hit] = False
+    assert np.array_equal(good[others].view(np.uint32), y[others].view(np.uint32))
+    assert np.all(np.isfinite(y[rows_hit]))
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("fmt", ["coo", "csr0", "csr1", "csr2", "ell"])
 def test_load_widths_agree(oracle_lib, fmt, dtype):
