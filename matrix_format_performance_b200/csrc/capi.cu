@@ -30,6 +30,11 @@ int cuda_fail(cudaError_t e, const char *what) {
     if (_e != cudaSuccess) return cuda_fail(_e, what); \
   } while (0)
 
+// COO, the hybrid's tail and row-ordered SCOO keep their rows in handles as
+// 16-bit offsets where they fit (1), or always as 32-bit ids (0).
+#ifndef MFP_COMPACT_ROWS
+#define MFP_COMPACT_ROWS 1
+#endif
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 inline bool aligned32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
 // Per-lane group loads of the warp-tile kernels: 2 = one 32-byte load per
@@ -704,7 +709,8 @@ cudaError_t launch_after(void (*k)(KArgs...), uint32_t grid, cudaStream_t s, Arg
 
 template <typename T, bool ACCUM = false>
 int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
-             const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
+             const T *x, T *y, void *ws, size_t ws_bytes, void *stream, const uint16_t *rel = nullptr,
+             const uint32_t *tile_base = nullptr) {
   if (rows == 0) return ok();
   if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
   if (nnz == 0) return ACCUM ? ok() : fill<T>(rows, y, T(0), stream);
@@ -723,14 +729,18 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
   const int vec = vec_level(data, cols, rids);
   cudaStream_t s = as_stream(stream);
-  auto k = vec == 2 ? d::coo_warp_kernel<T, 2, ACCUM>
-                    : (vec == 1 ? d::coo_warp_kernel<T, 1, ACCUM> : d::coo_warp_kernel<T, 0, ACCUM>);
+  // compact 16-bit rows (handles) on 32-byte-aligned arrays
+  const bool r16 = rel && tile_base && vec == 2 && aligned16(rel);
+  auto k = r16 ? d::coo_warp_kernel<T, 2, ACCUM, true>
+               : (vec == 2 ? d::coo_warp_kernel<T, 2, ACCUM>
+                           : (vec == 1 ? d::coo_warp_kernel<T, 1, ACCUM> : d::coo_warp_kernel<T, 0, ACCUM>));
+  if (!r16) rel = nullptr, tile_base = nullptr;
   // the accumulating warp pass (hybrid tail) follows the ELL launch of the same call
   cudaError_t e;
   if (ACCUM)
-    e = launch_after(k, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr);
+    e = launch_after(k, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base);
   else {
-    k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr);
+    k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) return cuda_fail(e, "coo_warp_kernel launch");
@@ -775,16 +785,25 @@ int csr_tile_spmv(const mfp_csr_plan *plan, const T *data, const uint32_t *cols,
   return ok();
 }
 
-template <typename T, int VEC, bool XWIN, bool UNSORTED = false>
+template <typename T, int VEC, bool XWIN, bool UNSORTED = false, bool R16 = false>
 int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32_t slice, const T *v,
                 const uint32_t *ci, const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw,
-                const uint32_t *order, const T *x, T *y) {
-  auto k = UNSORTED ? d::scoo_unsorted_kernel<T, XWIN> : d::scoo_kernel<T, VEC, XWIN>;
-  if (dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
-    const int st = ensure_dyn_smem((const void *)k, dyn, "scoo_kernel");
-    if (st) return st;
+                const uint32_t *order, const T *x, T *y, const uint16_t *rel = nullptr) {
+  if (UNSORTED) {
+    auto k = d::scoo_unsorted_kernel<T, XWIN>;
+    if (dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
+      const int st = ensure_dyn_smem((const void *)k, dyn, "scoo_kernel");
+      if (st) return st;
+    }
+    k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  } else {
+    auto k = d::scoo_kernel<T, VEC, XWIN, R16>;
+    if (dyn > 48 * 1024 - sizeof(d::scoo_smem_static<T>)) {
+      const int st = ensure_dyn_smem((const void *)k, dyn, "scoo_kernel");
+      if (st) return st;
+    }
+    k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, order, x, y, rel);
   }
-  k<<<grid, d::kBlock, dyn, s>>>(rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return fail(MFP_ERROR_CUDA, "scoo_kernel launch (grid %u, %zu dynamic bytes): %s", grid, dyn, cudaGetErrorString(e));
@@ -794,7 +813,7 @@ int scoo_launch(uint32_t grid, size_t dyn, cudaStream_t s, uint32_t rows, uint32
 template <typename T, bool UNSORTED = false>
 int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const uint32_t *ci,
               const uint32_t *ri, const uint32_t *sp, const uint32_t *win, uint32_t maxw, const uint32_t *order,
-              const T *x, T *y, void *stream) {
+              const T *x, T *y, void *stream, const uint16_t *rel = nullptr) {
   if (rows == 0) return ok();
   // values / c_index / r_index may be NULL only when every slice is empty
   if (!y || !sp || !x) return fail(MFP_ERROR_INVALID_VALUE, "null device array");
@@ -809,6 +828,13 @@ int scoo_spmv(uint32_t rows, uint32_t slices, uint32_t slice, const T *v, const 
   if (UNSORTED) {
     if (win) return scoo_launch<T, 0, true, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
     return scoo_launch<T, 0, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
+  }
+  if (vec == 2 && rel && aligned16(rel)) {  // compact 16-bit rows (handles)
+    if (win)
+      return scoo_launch<T, 2, true, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y,
+                                                  rel);
+    return scoo_launch<T, 2, false, false, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y,
+                                                 rel);
   }
   if (vec == 2) {
     if (win) return scoo_launch<T, 2, true>(slices, dyn, s, rows, slice, v, ci, ri, sp, win, maxw, order, x, y);
@@ -942,13 +968,14 @@ int lowp_ell_spmv(int vt, uint32_t rows, uint32_t cols_n, uint32_t width, const 
 // kernel adds the tail (elements past the ELL width) row by row.
 template <typename T>
 int hyb_spmv(uint32_t rows, uint32_t width, const T *ed, const uint32_t *ec, uint32_t cnnz, const T *cd,
-             const uint32_t *cc, const uint32_t *cr, const T *x, T *y, void *ws, size_t ws_bytes, void *stream) {
+             const uint32_t *cc, const uint32_t *cr, const T *x, T *y, void *ws, size_t ws_bytes, void *stream,
+             const uint16_t *rel = nullptr, const uint32_t *tile_base = nullptr) {
   if (rows == 0) return ok();
   if (!y || !x || (width && (!ed || !ec)) || (cnnz && (!cd || !cc || !cr)))
     return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   int st = ell_spmv<T>(rows, width, ed, ec, x, y, stream);
   if (st) return st;
-  return coo_spmv<T, true>(rows, cnnz, cd, cc, cr, x, y, ws, ws_bytes, stream);
+  return coo_spmv<T, true>(rows, cnnz, cd, cc, cr, x, y, ws, ws_bytes, stream, rel, tile_base);
 }
 }  // namespace
 
@@ -1185,6 +1212,11 @@ struct mfp_matrix {
   mfp_csr_plan *plan = nullptr;
   void *ws = nullptr;
   size_t ws_bytes = 0;
+  // compact rows (COO, the hybrid's tail, row-ordered SCOO): 16-bit offsets
+  // from each 256-element tile's first row (tile_base), or from the slice's
+  // first row for SCOO; NULL when some offset needs more than 16 bits
+  uint16_t *rel = nullptr;
+  uint32_t *tile_base = nullptr;
   void *dx = nullptr, *dy = nullptr;  // staging for the host-buffer call
   // second staging pair, copy streams and events of the pipelined host-buffer
   // call (made on its first use)
@@ -1220,8 +1252,56 @@ int track_upload_bytes(mfp_matrix *m, void **p, const void *host, size_t bytes) 
   *p = q;
   return st;
 }
+// Compact rows for the COO-family handles: 16-bit offsets built on the device
+// from the uploaded 32-bit rows.  Kept only when every offset fits; the
+// format's byte count then charges 2 bytes per row id (and 4 per tile base).
+int attach_compact_rows(mfp_matrix *m) {
+  const bool coo = m->format == MFP_FORMAT_COO, hyb = m->format == MFP_FORMAT_HYBRID;
+  const bool scoo = m->format == MFP_FORMAT_SCOO && !m->rows_unsorted;
+  const uint32_t n = coo ? (uint32_t)m->nnz : hyb ? m->coo_nnz : scoo ? (uint32_t)m->nnz : 0u;
+  const uint32_t *rows = hyb ? m->rows2 : m->rows_a;
+  if (!MFP_COMPACT_ROWS || n == 0 || !rows || (scoo && m->slice_size > 65536u)) return ok();
+  const uint32_t tiles = ceil_div(n, d::kWarpTile);
+  uint16_t *rel = nullptr;
+  uint32_t *base = nullptr, *flag = nullptr;
+  int st = dmalloc(&rel, n, nullptr);
+  if (!st && !scoo) st = dmalloc(&base, tiles, nullptr);
+  if (!st) st = dmalloc(&flag, 1, nullptr);
+  uint32_t hflag = 1;
+  if (!st && cudaMemset(flag, 0, sizeof(uint32_t)) != cudaSuccess) st = fail(MFP_ERROR_CUDA, "cudaMemset");
+  if (!st) {
+    if (scoo)
+      d::scoo_rows16_kernel<<<m->slices, d::kBlock>>>(m->slice_size, m->aux, rows, rel, flag);
+    else
+      d::coo_rows16_kernel<<<ceil_div(n, d::kBlock), d::kBlock>>>(n, rows, base, rel, flag);
+    if (cudaMemcpy(&hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  cudaFree(flag);
+  if (st || hflag) {  // an offset does not fit: 32-bit rows
+    cudaFree(rel);
+    cudaFree(base);
+    return st;
+  }
+  m->rel = rel;
+  m->tile_base = base;
+  m->allocs.push_back(rel);
+  if (base) m->allocs.push_back(base);
+  m->device_bytes += (size_t)n * 2 + (base ? (size_t)tiles * 4 : 0);
+  m->format_bytes -= (uint64_t)n * 2;
+  if (base) m->format_bytes += (uint64_t)tiles * 4;
+  return ok();
+}
+
 int finish_matrix(mfp_matrix *m, mfp_matrix **out) {
   const size_t vs = value_size(m->value_type);
+  {
+    const int st0 = attach_compact_rows(m);
+    if (st0) {
+      mfp_matrix_destroy(m);
+      return st0;
+    }
+  }
   int st = track_upload_bytes(m, &m->dx, nullptr, 0);
   unsigned char *a = nullptr, *b = nullptr;
   if (!st) st = track(m, &a, (size_t)std::max(1u, m->cols) * vs);
@@ -1749,9 +1829,9 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                                    (float *)y, stream);
     case MFP_FORMAT_COO:
       return f64 ? coo_spmv<double>(m->rows, (uint32_t)m->nnz, (const double *)m->vals, m->cols_a, m->rows_a,
-                                    (const double *)x, (double *)y, m->ws, m->ws_bytes, stream)
+                                    (const double *)x, (double *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base)
                  : coo_spmv<float>(m->rows, (uint32_t)m->nnz, (const float *)m->vals, m->cols_a, m->rows_a,
-                                   (const float *)x, (float *)y, m->ws, m->ws_bytes, stream);
+                                   (const float *)x, (float *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base);
     case MFP_FORMAT_SCOO:
       if (m->rows_unsorted)
         return f64 ? scoo_spmv<double, true>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
@@ -1762,16 +1842,17 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                                             (float *)y, stream);
       return f64 ? scoo_spmv<double>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
                                      m->rows_a, m->aux, m->win, m->max_window, m->order, (const double *)x,
-                                     (double *)y, stream)
+                                     (double *)y, stream, m->rel)
                  : scoo_spmv<float>(m->rows, m->slices, m->slice_size, (const float *)m->vals, m->cols_a, m->rows_a,
-                                    m->aux, m->win, m->max_window, m->order, (const float *)x, (float *)y, stream);
+                                    m->aux, m->win, m->max_window, m->order, (const float *)x, (float *)y, stream,
+                                    m->rel);
     case MFP_FORMAT_HYBRID:
       return f64 ? hyb_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, m->coo_nnz,
                                     (const double *)m->vals2, m->cols2, m->rows2, (const double *)x, (double *)y,
-                                    m->ws, m->ws_bytes, stream)
+                                    m->ws, m->ws_bytes, stream, m->rel, m->tile_base)
                  : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
                                    (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
-                                   m->ws_bytes, stream);
+                                   m->ws_bytes, stream, m->rel, m->tile_base);
     case MFP_FORMAT_ELL_LOWP:
       return lowp_ell_spmv(m->lowp_vt, m->rows, m->cols, m->width, (const uint16_t *)m->vals, m->scale,
                            m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);

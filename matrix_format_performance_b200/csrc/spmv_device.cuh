@@ -76,6 +76,18 @@ __device__ __forceinline__ void ld_stream8(const uint32_t *p, uint32_t (&v)[8], 
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                : "l"(p), "l"(pol));
 }
+// 16-bit words: 8 (16 bytes, p 16-byte aligned, packed two per register) or one.
+__device__ __forceinline__ void ld_stream8_u16(const uint16_t *p, uint32_t (&w)[4], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+               : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t *p, uint64_t pol) {
+  unsigned short v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // 32-byte store (p 32-byte aligned).
 __device__ __forceinline__ void st_global8(float *p, const float (&v)[8]) {
   asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),

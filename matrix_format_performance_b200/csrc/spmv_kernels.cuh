@@ -1180,11 +1180,81 @@ __device__ __forceinline__ void warp_tile_reduce(uint32_t wt, uint32_t g0, uint3
   }
 }
 
-template <typename T, int VEC, bool ACCUM>
+// A group of 8 elements whose rows are 16-bit offsets rel from a base row
+// (compact COO / SCOO rows, 2 bytes per element instead of 4).  As
+// load_run_group, with one 32-byte load per array for vals and cols (VEC 2)
+// and one 16-byte load for the offsets.
+template <typename T, int VEC, typename XS>
+__device__ __forceinline__ uint32_t load_run_group16(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                                     const uint16_t *__restrict__ rel, uint32_t base, XS xs,
+                                                     uint32_t g, uint32_t c0, uint32_t c1, T (&p)[kEpt],
+                                                     uint32_t (&r)[kEpt], uint32_t &i0, uint64_t pol) {
+  i0 = max(g, c0);
+  const uint32_t i1 = min(g + kEpt, c1);
+  if (i0 >= i1) return 0u;
+  const uint32_t cnt = i1 - i0;
+  if (VEC == 2 && cnt == kEpt) {
+    T v[8];
+    uint32_t k[8], w[4];
+    ld_stream8(vals + i0, v, pol);
+    ld_stream8(cols + i0, k, pol);
+    ld_stream8_u16(rel + i0, w, pol);
+    T xv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xv[j] = xs(k[j]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      p[j] = mul_rn(v[j], xv[j]);
+      r[j] = base + ((j & 1) ? (w[j >> 1] >> 16) : (w[j >> 1] & 0xffffu));
+    }
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < kEpt; ++k) {
+      if (k < cnt) {
+        const uint32_t e = i0 + k;
+        r[k] = base + ld_stream_u16(rel + e, pol);
+        p[k] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+      }
+    }
+  }
+  return cnt;
+}
+
+// Compact COO rows: rows[e] - rows[first element of e's 256-element tile],
+// and that first row per tile; *flag |= 1 when a tile spans more than 65,535
+// rows (the layout then keeps 32-bit rows).  rows sorted.
+__global__ void coo_rows16_kernel(uint32_t nnz, const uint32_t *__restrict__ rows, uint32_t *__restrict__ tile_base,
+                                  uint16_t *__restrict__ rel, uint32_t *flag) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nnz) return;
+  const uint32_t t = e / kWarpTile;
+  const uint32_t base = rows[t * kWarpTile];
+  const uint32_t d = rows[e] - base;
+  if (e % kWarpTile == 0) tile_base[t] = base;
+  if (d > 0xffffu) atomicOr(flag, 1u);
+  rel[e] = (uint16_t)d;
+}
+
+// Compact SCOO rows: r_index[e] - s * slice_size for the elements of slice s
+// (one CTA per slice); *flag |= 1 when an offset exceeds 65,535.
+__global__ void scoo_rows16_kernel(uint32_t slice_size, const uint32_t *__restrict__ slices_ptr,
+                                   const uint32_t *__restrict__ rows, uint16_t *__restrict__ rel, uint32_t *flag) {
+  const uint32_t s = blockIdx.x;
+  const uint32_t row0 = s * slice_size;
+  for (uint32_t e = slices_ptr[s] + threadIdx.x; e < slices_ptr[s + 1]; e += blockDim.x) {
+    const uint32_t d = rows[e] - row0;
+    if (d > 0xffffu) atomicOr(flag, 1u);
+    rel[e] = (uint16_t)d;
+  }
+}
+
+// R16: rows as 16-bit offsets rel from tile_base[tile] (compact COO rows).
+template <typename T, int VEC, bool ACCUM, bool R16 = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
-                    coo_carry<T> cw, coo_ws_header *hdr) {
+                    coo_carry<T> cw, coo_ws_header *hdr, const uint16_t *__restrict__ rel = nullptr,
+                    const uint32_t *__restrict__ tile_base = nullptr) {
   if (ACCUM) griddep_wait();  // y holds the ELL part written by the preceding launch
   const uint64_t pol = policy_evict_first();
   const uint32_t lane = threadIdx.x & 31u;
@@ -1193,10 +1263,17 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
   const uint32_t c0 = wt * kWarpTile, c1 = min(nnz, c0 + kWarpTile);
   T pr[kEpt];
   uint32_t rw[kEpt], i0 = 0;
-  const uint32_t cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + lane * kEpt, c0, c1, pr, rw,
-                                              i0, pol);
-  const uint32_t prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
-  const uint32_t nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
+  uint32_t cnt, prv, nxt;
+  if (R16) {
+    cnt = load_run_group16<T, VEC>(vals, cols, rel, __ldg(tile_base + wt), x_global<T>{x}, c0 + lane * kEpt, c0, c1,
+                                   pr, rw, i0, pol);
+    prv = c0 > 0 ? __ldg(tile_base + wt - 1u) + ld_stream_u16(rel + c0 - 1u, pol) : kNoRow;  // row before the tile
+    nxt = c1 < nnz ? __ldg(tile_base + wt + 1u) : kNoRow;  // row after the tile: the next tile's base
+  } else {
+    cnt = load_run_group<T, VEC>(vals, cols, rows, x_global<T>{x}, c0 + lane * kEpt, c0, c1, pr, rw, i0, pol);
+    prv = c0 > 0 ? __ldg(rows + c0 - 1u) : kNoRow;  // row before the tile
+    nxt = c1 < nnz ? __ldg(rows + c1) : kNoRow;     // row after the tile
+  }
   warp_tile_reduce<T, ACCUM>(wt, c0, c1, nnz, n_rows, pr, rw, cnt, prv, nxt, y, cw, hdr);
 }
 
@@ -1438,7 +1515,9 @@ struct scoo_smem_static {
   };
 };
 
-template <typename T, int VEC, bool XWIN>
+// R16: rel holds each element's row as a 16-bit offset from its slice's
+// first row (compact SCOO rows; ridx stays for the whole-CTA chunk path).
+template <typename T, int VEC, bool XWIN, bool R16 = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : MFP_COO_MINBLOCKS64) scoo_kernel(uint32_t n_rows, uint32_t slice_size,
                                                       const T *__restrict__ vals,
                                                       const uint32_t *__restrict__ cidx,
@@ -1447,7 +1526,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
                                                       const uint32_t *__restrict__ windows,
                                                       uint32_t max_window,
                                                       const uint32_t *__restrict__ order,
-                                                      const T *__restrict__ x, T *__restrict__ y) {
+                                                      const T *__restrict__ x, T *__restrict__ y,
+                                                      const uint16_t *__restrict__ rel = nullptr) {
   __shared__ scoo_smem_static<T> sm;
   extern __shared__ __align__(16) unsigned char dyn[];
   T *acc = reinterpret_cast<T *>(dyn);                       // slice_size (rounded to 4)
@@ -1495,13 +1575,22 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_SCOO_MINBLOCKS : 
         T pr[kEpt];
         uint32_t rw[kEpt], i0 = 0;
         const uint32_t g = g0 + lane * kEpt;
-        const uint32_t cnt =
-            (XWIN && use_win) ? load_run_group<T, VEC>(vals, cidx, ridx, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
-                              : load_run_group<T, VEC>(vals, cidx, ridx, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
+        uint32_t cnt, prv, nxt;
+        if (R16) {  // the offsets are the slice-local rows
+          cnt = (XWIN && use_win)
+                    ? load_run_group16<T, VEC>(vals, cidx, rel, 0u, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
+                    : load_run_group16<T, VEC>(vals, cidx, rel, 0u, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
+          prv = c0 > eb ? ld_stream_u16(rel + c0 - 1u, pol) : kNoRow;
+          nxt = c1 < ee ? ld_stream_u16(rel + c1, pol) : kNoRow;
+        } else {
+          cnt = (XWIN && use_win)
+                    ? load_run_group<T, VEC>(vals, cidx, ridx, x_window<T>{s_x, wlo}, g, c0, c1, pr, rw, i0, pol)
+                    : load_run_group<T, VEC>(vals, cidx, ridx, x_global<T>{x}, g, c0, c1, pr, rw, i0, pol);
 #pragma unroll
-        for (int k = 0; k < kEpt; ++k) rw[k] -= row0;
-        const uint32_t prv = c0 > eb ? __ldg(ridx + c0 - 1u) - row0 : kNoRow;
-        const uint32_t nxt = c1 < ee ? __ldg(ridx + c1) - row0 : kNoRow;
+          for (int k = 0; k < kEpt; ++k) rw[k] -= row0;
+          prv = c0 > eb ? __ldg(ridx + c0 - 1u) - row0 : kNoRow;
+          nxt = c1 < ee ? __ldg(ridx + c1) - row0 : kNoRow;
+        }
         warp_tile_reduce<T, true>(t, g0, c1, ee, nrows, pr, rw, cnt, prv, nxt, acc, cw, nullptr);
       }
       __syncthreads();

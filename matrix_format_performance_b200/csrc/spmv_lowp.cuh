@@ -51,16 +51,6 @@ __device__ __forceinline__ float2 lowp_pair(uint32_t w) {
   return __half22float2(h);
 }
 
-__device__ __forceinline__ void ld_stream8_u16(const uint16_t *p, uint32_t (&w)[4], uint64_t pol) {
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
-               : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
-               : "l"(p), "l"(pol));
-}
-__device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t *p, uint64_t pol) {
-  unsigned short v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
-  return v;
-}
 
 template <int VT, bool D16>
 struct lowp_args {

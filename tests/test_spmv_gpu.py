@@ -353,6 +353,92 @@ def test_scoo_tiles_and_chunk_fallback(oracle_lib, dtype):
     check_tol(oracle_lib, m, x, a, "scoo tiles / chunks")
 
 
+@pytest.mark.parametrize("fmt", [COO, SCOO, HYBRID])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_compact_rows_give_the_bits_of_32_bit_rows(oracle_lib, fmt, dtype):
+    """COO, SCOO and hybrid handles keep their rows as 16-bit offsets (from
+    each 256-element tile's first row, or the slice's first row): the same
+    bits as the raw entry points on the 32-bit row ids, and 2 bytes less
+    per row id in the handle's byte count."""
+    m = syn("power_law_300k").astype(dtype)
+    x = synth.vector(13, m.cols).astype(dtype)
+    xt = torch.from_numpy(x).cuda()
+    sfx = "f32" if dtype == np.float32 else "f64"
+    keep = []
+
+    def dev(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        keep.append(t)
+        return C.c_void_p(t.data_ptr())
+    yr = torch.full((m.rows,), float("nan"), dtype=xt.dtype, device="cuda")
+    vs = np.dtype(dtype).itemsize
+    if fmt == COO:
+        c = F.coo_matrix_class(m)
+        nbytes = C.c_size_t()
+        call("mfp_coo_workspace_bytes", m.rows, m.nnz, C.byref(nbytes))
+        ws = torch.zeros(nbytes.value, dtype=torch.uint8, device="cuda")
+        call(f"mfp_coo_spmv_{sfx}", m.rows, m.cols, m.nnz, dev(c.data), dev(c.cols_.view(np.int32)),
+             dev(c.rows_.view(np.int32)), C.c_void_p(xt.data_ptr()), C.c_void_p(yr.data_ptr()),
+             C.c_void_p(ws.data_ptr()), nbytes.value, None)
+        dm = DeviceMatrix.from_coo(c)
+        n_ids, tiles = m.nnz, -(-m.nnz // 256)
+    elif fmt == SCOO:
+        c = F.scoo_matrix_class(148, 49152, m)
+        call(f"mfp_scoo_spmv_{sfx}", m.rows, m.cols, c.slices_count, c.slice_size, dev(c.values),
+             dev(c.c_index.view(np.int32)), dev(c.r_index.view(np.int32)), dev(c.slices_ptr.view(np.int32)), None, 0,
+             None, C.c_void_p(xt.data_ptr()), C.c_void_p(yr.data_ptr()), None)
+        dm = DeviceMatrix.from_scoo(c)
+        n_ids, tiles = m.nnz, 0
+    else:
+        hm = F.hybrid_matrix_class(m)
+        hm.allocate_width(m, 2)
+        e, c = hm.ell_matrix, hm.coo_matrix
+        nbytes = C.c_size_t()
+        call("mfp_hybrid_workspace_bytes", m.rows, c.elements_count, C.byref(nbytes))
+        ws = torch.zeros(max(1, nbytes.value), dtype=torch.uint8, device="cuda")
+        call(f"mfp_hybrid_spmv_{sfx}", m.rows, m.cols, e.elements_in_rows, dev(e.data),
+             dev(e.columns.view(np.int32)), c.elements_count, dev(c.data), dev(c.cols_.view(np.int32)),
+             dev(c.rows_.view(np.int32)), C.c_void_p(xt.data_ptr()), C.c_void_p(yr.data_ptr()),
+             C.c_void_p(ws.data_ptr()), nbytes.value, None)
+        dm = DeviceMatrix.from_hybrid(hm)
+        n_ids, tiles = c.elements_count, -(-c.elements_count // 256)
+    torch.cuda.synchronize()
+    yh = torch.full((m.rows,), float("nan"), dtype=xt.dtype, device="cuda")
+    dm.spmv(xt, yh)
+    torch.cuda.synchronize()
+    info = dm.info()
+    dm.close()
+    assert np.array_equal(yr.cpu().numpy().view(np.uint8), yh.cpu().numpy().view(np.uint8))
+    check_tol(oracle_lib, m, x, yh.cpu().numpy(), "compact rows")
+    if fmt == COO:
+        assert info.format_bytes == m.nnz * (vs + 6) + 4 * tiles + m.cols * vs + m.rows * vs
+    elif fmt == SCOO:
+        assert info.format_bytes == m.nnz * (vs + 6) + (c.slices_count + 1) * 4 + m.cols * vs + m.rows * vs
+
+
+def test_compact_rows_fall_back_when_a_tile_spans_more_than_16_bits(oracle_lib):
+    """A COO tile whose rows span more than 65,535 (long runs of empty rows)
+    keeps 32-bit rows; the handle's y is right either way."""
+    rows, cols = 300_000, 1000
+    rng = np.random.default_rng(5)
+    r = np.sort(np.concatenate([rng.integers(0, 10, 200), [70_000, 150_000, 299_999], rng.integers(0, rows, 400)]))
+    lens = np.bincount(r, minlength=rows)
+    rp = np.zeros(rows + 1, np.uint32)
+    rp[1:] = np.cumsum(lens)
+    colv = np.concatenate([np.sort(rng.choice(cols, n, replace=False)) for n in lens if n]).astype(np.uint32)
+    m = F.csr_matrix_class.from_arrays(rows, cols, rp, colv, rng.uniform(-1, 1, len(colv)), np.float32)
+    x = synth.vector(3, cols).astype(np.float32)
+    dm = DeviceMatrix.build(m, COO)
+    info = dm.info()
+    xt = torch.from_numpy(x).cuda()
+    y = torch.full((rows,), float("nan"), device="cuda")
+    dm.spmv(xt, y)
+    torch.cuda.synchronize()
+    dm.close()
+    assert info.format_bytes == m.nnz * 12 + cols * 4 + rows * 4  # 32-bit rows kept
+    check_tol(oracle_lib, m, x, y.cpu().numpy(), "coo fallback rows")
+
+
 def test_raw_scoo_row_ids_outside_their_slice_stay_in_bounds(oracle_lib):
     """mfp_scoo_spmv_f32 on caller arrays where one element's row id points
     into the previous slice (inside a long row the warp tiles carry across
