@@ -37,6 +37,8 @@ lowp         BF16 / FP16 values with per-row scales (CSR with 16-bit column
              the engine's FP64 CSR kernel, which the tests hold to 1e-12)
 load_ceiling the load probe (mfp_probe_spmv_loads) on power_law_4M: the
              time of the SpMV's loads alone, a floor for every format
+hybrid_widths the power-law hybrid at the headline's 2/3-quantile ELL width
+             and at the width that moves the fewest bytes
 
 --impl reference times the reference's own CPU loop
 (cpu_csr_spmv_single_thread_naive, compiled from its sources into
@@ -272,6 +274,20 @@ def measure_plain(name, m, formats, steps, warmup, flush, stream, peak, hybrid_w
     del rp, ci, va
     return {"rows": m.rows, "cols": m.cols, "nnz": int(m.nnz), "algorithmic_bytes": int(nbytes),
             "formats": out, "fastest": min(out, key=lambda k: out[k]["ms"])}
+
+
+def byte_model_width(m, vs: int, row_bytes: int = 2, cap: int = 64) -> int:
+    """The hybrid ELL width that moves the fewest bytes: w slots of (value,
+    column) for every row against (value, column, row offset) for each tail
+    element past w, plus one 4-byte base per 256-element tile of the tail."""
+    lens = np.diff(m.row_ptr.astype(np.int64))
+    best, best_b = 0, None
+    for w in range(0, min(cap, int(lens.max())) + 1):
+        tail = int(np.maximum(lens - w, 0).sum())
+        b = w * m.rows * (vs + 4) + tail * (vs + 4 + row_bytes) + (tail + 255) // 256 * 4
+        if best_b is None or b < best_b:
+            best, best_b = w, b
+    return best
 
 
 def fp64_product(m64, x32):
@@ -579,7 +595,8 @@ def run_engine(args):
 
 def run_extras(args, power_law, x, per_format, flush, stream, peak, hyb_w):
     """The rest of the metric on one GPU: stencil / banded per format, FP64,
-    reduced precision, and the load ceiling of the power-law matrix."""
+    reduced precision, the load ceiling of the power-law matrix and its
+    hybrid at the byte model's ELL width."""
     from matrix_format_performance_b200 import formats as F
     from matrix_format_performance_b200 import synth
     from matrix_format_performance_b200.device import (COO, CSR_ADAPTIVE, CSR_SCALAR, CSR_VECTOR, ELL, HYBRID,
@@ -593,6 +610,18 @@ def run_extras(args, power_law, x, per_format, flush, stream, peak, hyb_w):
     res["load_ceiling"] = {"power_law_4M": measure_load_ceiling(power_law, steps, warmup, flush, stream, peak,
                                                                 best_pl)}
     log(f"[bench] load ceiling in {time.time() - t:.1f}s")
+    # the hybrid at the byte model's ELL width beside the 2/3-quantile width of
+    # the headline (the reference's own sweep varies the width too)
+    t = time.time()
+    wb = byte_model_width(power_law, 4)
+    hw = {"quantile_width": hyb_w, "byte_model_width": wb,
+          "note": "byte model: w*rows*(4+4) + tail*(4+4+2) + tail tiles*4 bytes, minimised over w"}
+    for label, w in (("quantile", hyb_w), ("byte_model", wb)):
+        e = measure_plain("power_law_4M", power_law, [HYBRID], steps, warmup, flush, stream, peak, w)
+        hw[label] = e["formats"]["GPU Hybrid (atomic)"]
+        hw[label]["format_bytes_over_algorithmic"] = round(hw[label]["format_bytes"] / e["algorithmic_bytes"], 3)
+    res["hybrid_widths"] = {"power_law_4M": hw}
+    log(f"[bench] hybrid widths in {time.time() - t:.1f}s")
     pl64 = synth.power_law(seed=0)
     t = time.time()
     res["fp64"]["power_law_4M"] = measure_plain("power_law_4M", pl64, no_ell, steps, warmup, flush, stream, peak,
