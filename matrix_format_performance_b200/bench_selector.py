@@ -13,7 +13,7 @@
    mfp_matrix_time median of 5 launches, L2 flushed before each).  Training
    seeds 0..train-1, held-out seeds 1,000,000 + i, and a second held-out set
    at the configuration's full sizes (seeds 2,000,000 + i, nonzeros up to
-   --big-cap) on which the selector is judged as is and with its sweep
+   --big-cap) on which the selector is evaluated as is and with its sweep
    fallback for features outside the training range.
 2. Training: an ensemble of MLPs 12-64-64-28 (--members, seeds 0, 1, ...)
    on the engine's CUDA kernels (Adam, masked MSE on log(time / best)); the

@@ -17,9 +17,9 @@ pattern (mfp_selector_features):
   mfp_mlp_backward / mfp_mlp_adam), against times the engine measured on
   seeded synthetic matrices, with a masked mean-squared error;
 - **fallback**: when a matrix's features lie outside the range seen in
-  training (or select(..., sweep=True) is asked for), the selector runs the
-  exhaustive sweep;
-- **regret**: the same sweep judges the selector's regret on held-out
+  training, select() runs the exhaustive sweep (sweep_if_unsure=False turns
+  this off);
+- **regret**: the same sweep measures the selector's regret on held-out
   matrices.
 """
 from __future__ import annotations
