@@ -1255,41 +1255,51 @@ int track_upload_bytes(mfp_matrix *m, void **p, const void *host, size_t bytes) 
 // Compact rows for the COO-family handles: 16-bit offsets built on the device
 // from the uploaded 32-bit rows.  Kept only when every offset fits; the
 // format's byte count then charges 2 bytes per row id (and 4 per tile base).
+// the fit flag of the compact-row conversion (one conversion at a time)
+__device__ uint32_t g_rows16_flag;
+std::mutex g_rows16_mu;
+
 int attach_compact_rows(mfp_matrix *m) {
   const bool coo = m->format == MFP_FORMAT_COO, hyb = m->format == MFP_FORMAT_HYBRID;
   const bool scoo = m->format == MFP_FORMAT_SCOO && !m->rows_unsorted;
   const uint32_t n = coo ? (uint32_t)m->nnz : hyb ? m->coo_nnz : scoo ? (uint32_t)m->nnz : 0u;
   const uint32_t *rows = hyb ? m->rows2 : m->rows_a;
   if (!MFP_COMPACT_ROWS || n == 0 || !rows || (scoo && m->slice_size > 65536u)) return ok();
-  const uint32_t tiles = ceil_div(n, d::kWarpTile);
-  uint16_t *rel = nullptr;
-  uint32_t *base = nullptr, *flag = nullptr;
-  int st = dmalloc(&rel, n, nullptr);
-  if (!st && !scoo) st = dmalloc(&base, tiles, nullptr);
-  if (!st) st = dmalloc(&flag, 1, nullptr);
+  const uint32_t tiles = scoo ? 0u : ceil_div(n, d::kWarpTile);
+  // one allocation: the offsets, then (16-byte aligned) the tile bases
+  const size_t rel_bytes = ((size_t)n * 2 + 15) & ~(size_t)15;
+  unsigned char *blk = nullptr;
+  int st = dmalloc(&blk, rel_bytes + (size_t)tiles * 4, nullptr);
+  if (st) return st;
+  uint16_t *rel = reinterpret_cast<uint16_t *>(blk);
+  uint32_t *base = tiles ? reinterpret_cast<uint32_t *>(blk + rel_bytes) : nullptr;
   uint32_t hflag = 1;
-  if (!st && cudaMemset(flag, 0, sizeof(uint32_t)) != cudaSuccess) st = fail(MFP_ERROR_CUDA, "cudaMemset");
-  if (!st) {
-    if (scoo)
-      d::scoo_rows16_kernel<<<m->slices, d::kBlock>>>(m->slice_size, m->aux, rows, rel, flag);
-    else
-      d::coo_rows16_kernel<<<ceil_div(n, d::kBlock), d::kBlock>>>(n, rows, base, rel, flag);
-    if (cudaMemcpy(&hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+  {
+    std::lock_guard<std::mutex> g(g_rows16_mu);
+    uint32_t *flag = nullptr;
+    const uint32_t zero = 0;
+    if (cudaGetSymbolAddress(reinterpret_cast<void **>(&flag), g_rows16_flag) != cudaSuccess ||
+        cudaMemcpy(flag, &zero, sizeof(zero), cudaMemcpyHostToDevice) != cudaSuccess) {
       st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+    } else {
+      if (scoo)
+        d::scoo_rows16_kernel<<<m->slices, d::kBlock>>>(m->slice_size, m->aux, rows, rel, flag);
+      else
+        d::coo_rows16_kernel<<<ceil_div(n, d::kBlock), d::kBlock>>>(n, rows, base, rel, flag);
+      if (cudaMemcpy(&hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+    }
   }
-  cudaFree(flag);
   if (st || hflag) {  // an offset does not fit: 32-bit rows
-    cudaFree(rel);
-    cudaFree(base);
+    cudaFree(blk);
     return st;
   }
   m->rel = rel;
   m->tile_base = base;
-  m->allocs.push_back(rel);
-  if (base) m->allocs.push_back(base);
-  m->device_bytes += (size_t)n * 2 + (base ? (size_t)tiles * 4 : 0);
+  m->allocs.push_back(blk);
+  m->device_bytes += rel_bytes + (size_t)tiles * 4;
   m->format_bytes -= (uint64_t)n * 2;
-  if (base) m->format_bytes += (uint64_t)tiles * 4;
+  m->format_bytes += (uint64_t)tiles * 4;
   return ok();
 }
 

@@ -11,7 +11,7 @@ pattern (mfp_selector_features):
   configurations the matrix admits; with verify=k it times the k smallest
   on the matrix (k of the 28 configurations) and takes the fastest, which
   absorbs the network's near-ties (on the measured held-out set: within 5%
-  of the best for 86% of the matrices from the prediction alone, 95% with
+  of the best for 84% of the matrices from the prediction alone, 95.5% with
   the three best predictions timed);
 - **training**: on the engine's own kernels (mfp_mlp_forward /
   mfp_mlp_backward / mfp_mlp_adam), against times the engine measured on
@@ -39,8 +39,10 @@ N_FEATURES, N_HIDDEN, N_OUT = 12, 64, 28
 # (format name, config) per output slot; None = no such configuration of that
 # format (masked in training and never selected).
 CONFIGS: list[tuple[str, dict] | None] = [
-    # CSR scalar: warp-assist / long-row thresholds, and the streaming kernel
-    ("csr", {"kernel": 1}), ("csr", {"kernel": 1, "assist_threshold": 32}),
+    # CSR scalar: the automatic kernel (element-balanced bins below a mean row
+    # length of 16), the row blocks at two warp-assist / long-row thresholds,
+    # and the streaming kernel
+    ("csr", {}), ("csr", {"kernel": 1}),
     ("csr", {"kernel": 1, "assist_threshold": 256, "long_row_threshold": 16384}), ("csr", {"kernel": 2}),
     # CSR vector: lanes per row
     ("csr_vector", {}), ("csr_vector", {"vector_lanes": 4}), ("csr_vector", {"vector_lanes": 8}),
