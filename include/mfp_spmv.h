@@ -594,7 +594,9 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream);
  * When host_y is page-locked and device-addressable and the format's kernel
  * stores each row of y once in row order (CSR scalar / adaptive, CSR vector
  * with lanes per row, ELL, SCOO, the reduced-precision layouts), the kernel
- * stores y straight into host_y, so the copy-out overlaps the kernel. */
+ * stores y straight into host_y, so the copy-out overlaps the kernel.
+ * The host-buffer calls stage through buffers owned by the handle: one such
+ * call at a time per handle. */
 int mfp_matrix_spmv_host(mfp_matrix *m, const void *host_x, void *host_y, void *stream);
 /* count independent products host_y[i] = A*host_x[i] with HOST vectors,
  * pipelined: x_{i+1} is copied in while SpMV i runs and y_{i-1} is copied
