@@ -8,7 +8,7 @@ profiler (ncu captures one launch per kernel with -k / -c).
 Matrices: power_law (Zipf(2.0) row lengths, --rows rows), stencil (27-point,
 --n^3 rows), banded (--rows rows, 32 per row in a half band of 64).  Formats:
 csr, csr_vector, csr_adaptive, ell, coo, scoo, hybrid (ELL width at the
-2/3-quantile), ell_bf16 / csr_bf16 (16-bit values, 16-bit indices), probe
+2/3-quantile, or --hybrid-width), ell_bf16 / csr_bf16 (16-bit values, 16-bit indices), probe
 (mfp_probe_spmv_loads mode 2).  Every layout is converted on the GPU from one
 device CSR.  Prints one line with the matrix size when done.
 """
@@ -28,6 +28,7 @@ def main() -> None:
     ap.add_argument("--formats", default="csr,csr_vector,coo")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--hybrid-width", type=int, default=None, help="hybrid ELL width (default: 2/3-quantile)")
     a = ap.parse_args()
     import torch
 
@@ -66,7 +67,8 @@ def main() -> None:
             continue
         else:
             fmt = FORMAT_NAMES[name]
-            hw = F.row_length_quantile(m, 2 / 3) if fmt == HYBRID else None
+            hw = (a.hybrid_width if a.hybrid_width is not None else F.row_length_quantile(m, 2 / 3)) \
+                if fmt == HYBRID else None
             dm = DeviceMatrix.from_device_csr(rp, ci, va, m.cols, fmt, ell_width=hw)
             for _ in range(a.reps):
                 dm.spmv(x, y)
