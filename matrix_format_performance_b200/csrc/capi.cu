@@ -355,7 +355,9 @@ extern "C" int mfp_csr_plan_create(uint32_t rows, uint32_t cols, uint32_t nnz, c
   if (algo == MFP_CSR_ADAPTIVE || plan->binned)
     cfg.bin_nnz = cfg.bin_nnz ? std::min(cfg.bin_nnz, kMaxBin) : kMaxBin;
   if (algo == MFP_CSR_ADAPTIVE) {
-    if (cfg.long_row_threshold == 0) cfg.long_row_threshold = cfg.bin_nnz;
+    // rows longer than a bin and up to 4096 elements: one CTA each (plain
+    // float), longer ones in FP64 pieces
+    if (cfg.long_row_threshold == 0) cfg.long_row_threshold = std::max(cfg.bin_nnz, kDefaultLong);
   } else {
     if (cfg.long_row_threshold == 0) cfg.long_row_threshold = kDefaultLong;
   }
