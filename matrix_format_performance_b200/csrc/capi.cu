@@ -31,9 +31,13 @@ int cuda_fail(cudaError_t e, const char *what) {
   } while (0)
 
 // COO, the hybrid's tail and row-ordered SCOO keep their rows in handles as
-// 16-bit offsets where they fit (1), or always as 32-bit ids (0).
+// 16-bit offsets where they fit (1), or always as 32-bit ids (0); COO and the
+// hybrid's tail as 8-bit offsets where every tile allows them (ROWS8 1).
 #ifndef MFP_COMPACT_ROWS
 #define MFP_COMPACT_ROWS 1
+#endif
+#ifndef MFP_COMPACT_ROWS8
+#define MFP_COMPACT_ROWS8 1
 #endif
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 inline bool aligned32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
@@ -712,7 +716,7 @@ cudaError_t launch_after(void (*k)(KArgs...), uint32_t grid, cudaStream_t s, Arg
 template <typename T, bool ACCUM = false>
 int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, const uint32_t *rids,
              const T *x, T *y, void *ws, size_t ws_bytes, void *stream, const uint16_t *rel = nullptr,
-             const uint32_t *tile_base = nullptr) {
+             const uint32_t *tile_base = nullptr, const uint8_t *rel8 = nullptr, bool wide = false) {
   if (rows == 0) return ok();
   if (!y) return fail(MFP_ERROR_INVALID_VALUE, "null y");
   if (nnz == 0) return ACCUM ? ok() : fill<T>(rows, y, T(0), stream);
@@ -731,18 +735,23 @@ int coo_spmv(uint32_t rows, uint32_t nnz, const T *data, const uint32_t *cols, c
   const uint32_t grid = ceil_div(n_wt, d::kBlock / 32u);
   const int vec = vec_level(data, cols, rids);
   cudaStream_t s = as_stream(stream);
-  // compact 16-bit rows (handles) on 32-byte-aligned arrays
-  const bool r16 = rel && tile_base && vec == 2 && aligned16(rel);
-  auto k = r16 ? d::coo_warp_kernel<T, 2, ACCUM, true>
-               : (vec == 2 ? d::coo_warp_kernel<T, 2, ACCUM>
-                           : (vec == 1 ? d::coo_warp_kernel<T, 1, ACCUM> : d::coo_warp_kernel<T, 0, ACCUM>));
-  if (!r16) rel = nullptr, tile_base = nullptr;
+  // compact 8- or 16-bit rows (handles) on 32-byte-aligned arrays
+  const bool r8 = rel8 && tile_base && vec == 2 && aligned16(rel8);
+  const bool r16 = !r8 && rel && tile_base && vec == 2 && aligned16(rel);
+  auto k = r8    ? (wide ? d::coo_warp_kernel<T, 2, ACCUM, false, true, true>
+                         : d::coo_warp_kernel<T, 2, ACCUM, false, true>)
+           : r16 ? d::coo_warp_kernel<T, 2, ACCUM, true>
+                    : (vec == 2 ? d::coo_warp_kernel<T, 2, ACCUM>
+                                : (vec == 1 ? d::coo_warp_kernel<T, 1, ACCUM> : d::coo_warp_kernel<T, 0, ACCUM>));
+  if (!r16) rel = nullptr;
+  if (!r8) rel8 = nullptr;
+  if (!r8 && !r16) tile_base = nullptr;
   // the accumulating warp pass (hybrid tail) follows the ELL launch of the same call
   cudaError_t e;
   if (ACCUM)
-    e = launch_after(k, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base);
+    e = launch_after(k, grid, s, rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base, rel8);
   else {
-    k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base);
+    k<<<grid, d::kBlock, 0, s>>>(rows, nnz, data, cols, rids, x, y, cw, hdr, rel, tile_base, rel8);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) return cuda_fail(e, "coo_warp_kernel launch");
@@ -971,13 +980,14 @@ int lowp_ell_spmv(int vt, uint32_t rows, uint32_t cols_n, uint32_t width, const 
 template <typename T>
 int hyb_spmv(uint32_t rows, uint32_t width, const T *ed, const uint32_t *ec, uint32_t cnnz, const T *cd,
              const uint32_t *cc, const uint32_t *cr, const T *x, T *y, void *ws, size_t ws_bytes, void *stream,
-             const uint16_t *rel = nullptr, const uint32_t *tile_base = nullptr) {
+             const uint16_t *rel = nullptr, const uint32_t *tile_base = nullptr, const uint8_t *rel8 = nullptr,
+             bool wide = false) {
   if (rows == 0) return ok();
   if (!y || !x || (width && (!ed || !ec)) || (cnnz && (!cd || !cc || !cr)))
     return fail(MFP_ERROR_INVALID_VALUE, "null device array");
   int st = ell_spmv<T>(rows, width, ed, ec, x, y, stream);
   if (st) return st;
-  return coo_spmv<T, true>(rows, cnnz, cd, cc, cr, x, y, ws, ws_bytes, stream, rel, tile_base);
+  return coo_spmv<T, true>(rows, cnnz, cd, cc, cr, x, y, ws, ws_bytes, stream, rel, tile_base, rel8, wide);
 }
 }  // namespace
 
@@ -1214,11 +1224,14 @@ struct mfp_matrix {
   mfp_csr_plan *plan = nullptr;
   void *ws = nullptr;
   size_t ws_bytes = 0;
-  // compact rows (COO, the hybrid's tail, row-ordered SCOO): 16-bit offsets
-  // from each 256-element tile's first row (tile_base), or from the slice's
-  // first row for SCOO; NULL when some offset needs more than 16 bits
+  // compact rows (COO, the hybrid's tail, row-ordered SCOO): 16-bit (rel) or
+  // 8-bit (rel8) offsets from each 256-element tile's first row (tile_base),
+  // 16-bit from the slice's first row for SCOO; NULL when some offset needs
+  // more than 16 bits
   uint16_t *rel = nullptr;
   uint32_t *tile_base = nullptr;
+  uint8_t *rel8 = nullptr;  // COO / hybrid tail: 8-bit offsets (tiles of at most 256 rows)
+  uint32_t wide_tiles = 0;  // with rel8: tiles spanning more rows, which read rows_a / rows2
   void *dx = nullptr, *dy = nullptr;  // staging for the host-buffer call
   // second staging pair, copy streams and events of the pipelined host-buffer
   // call (made on its first use)
@@ -1254,11 +1267,12 @@ int track_upload_bytes(mfp_matrix *m, void **p, const void *host, size_t bytes) 
   *p = q;
   return st;
 }
-// Compact rows for the COO-family handles: 16-bit offsets built on the device
-// from the uploaded 32-bit rows.  Kept only when every offset fits; the
-// format's byte count then charges 2 bytes per row id (and 4 per tile base).
+// Compact rows for the COO-family handles: 8- or 16-bit offsets built on the
+// device from the uploaded 32-bit rows.  Kept only when every offset fits; the
+// format's byte count then charges 1 or 2 bytes per row id (and 4 per tile
+// base).
 // the fit flag of the compact-row conversion (one conversion at a time)
-__device__ uint32_t g_rows16_flag;
+__device__ uint32_t g_rows16_flag[2];
 std::mutex g_rows16_mu;
 
 int attach_compact_rows(mfp_matrix *m) {
@@ -1268,40 +1282,56 @@ int attach_compact_rows(mfp_matrix *m) {
   const uint32_t *rows = hyb ? m->rows2 : m->rows_a;
   if (!MFP_COMPACT_ROWS || n == 0 || !rows || (scoo && m->slice_size > 65536u)) return ok();
   const uint32_t tiles = scoo ? 0u : ceil_div(n, d::kWarpTile);
-  // one allocation: the offsets, then (16-byte aligned) the tile bases
-  const size_t rel_bytes = ((size_t)n * 2 + 15) & ~(size_t)15;
-  unsigned char *blk = nullptr;
-  int st = dmalloc(&blk, rel_bytes + (size_t)tiles * 4, nullptr);
-  if (st) return st;
-  uint16_t *rel = reinterpret_cast<uint16_t *>(blk);
-  uint32_t *base = tiles ? reinterpret_cast<uint32_t *>(blk + rel_bytes) : nullptr;
-  uint32_t hflag = 1;
-  {
-    std::lock_guard<std::mutex> g(g_rows16_mu);
-    uint32_t *flag = nullptr;
-    const uint32_t zero = 0;
-    if (cudaGetSymbolAddress(reinterpret_cast<void **>(&flag), g_rows16_flag) != cudaSuccess ||
-        cudaMemcpy(flag, &zero, sizeof(zero), cudaMemcpyHostToDevice) != cudaSuccess) {
-      st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
-    } else {
-      if (scoo)
-        d::scoo_rows16_kernel<<<m->slices, d::kBlock>>>(m->slice_size, m->aux, rows, rel, flag);
-      else
-        d::coo_rows16_kernel<<<ceil_div(n, d::kBlock), d::kBlock>>>(n, rows, base, rel, flag);
-      if (cudaMemcpy(&hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
-        st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
-    }
+  const uint32_t warp_grid = ceil_div(tiles, d::kBlock / 32u);
+  int st = 0;
+  uint32_t hflag[2] = {0, 0};
+  std::lock_guard<std::mutex> g(g_rows16_mu);
+  uint32_t *flag = nullptr;
+  const uint32_t zero[2] = {0, 0};
+  if (cudaGetSymbolAddress(reinterpret_cast<void **>(&flag), g_rows16_flag) != cudaSuccess ||
+      cudaMemcpy(flag, zero, sizeof(zero), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+  // the offsets' width: SCOO 16 bits (from the slice's first row); COO 8 bits
+  // when at most one tile in 8 spans more than 256 rows (those read the
+  // 32-bit rows; FP32 only: with FP64 values such tiles cost 3% on the
+  // power-law hybrid's tail), else 16 bits when every offset fits, else none
+  uint32_t w = 2;
+  if (!scoo) {
+    d::coo_rows_span_kernel<<<warp_grid, d::kBlock>>>(n, rows, flag);
+    if (cudaMemcpy(hflag, flag, sizeof(hflag), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+    if (MFP_COMPACT_ROWS8 && m->rows <= d::kWideTile && hflag[1] <= tiles / 8u &&
+        (hflag[1] == 0 || m->value_type == MFP_F32))
+      w = 1;
+    else if (hflag[0] & 1u) return ok();  // 32-bit rows
   }
-  if (st || hflag) {  // an offset does not fit: 32-bit rows
+  // one allocation: the offsets, then (16-byte aligned) the tile bases
+  const size_t rel_bytes = ((size_t)n * w + 15) & ~(size_t)15;
+  unsigned char *blk = nullptr;
+  if ((st = dmalloc(&blk, rel_bytes + (size_t)tiles * 4, nullptr))) return st;
+  uint32_t *base = tiles ? reinterpret_cast<uint32_t *>(blk + rel_bytes) : nullptr;
+  if (scoo)
+    d::scoo_rows16_kernel<<<m->slices, d::kBlock>>>(m->slice_size, m->aux, rows, reinterpret_cast<uint16_t *>(blk),
+                                                     flag);
+  else if (w == 1)
+    d::coo_rows8_kernel<<<warp_grid, d::kBlock>>>(n, rows, base, blk);
+  else
+    d::coo_rows16_kernel<<<ceil_div(n, d::kBlock), d::kBlock>>>(n, rows, base, reinterpret_cast<uint16_t *>(blk));
+  if (cudaMemcpy(hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = fail(MFP_ERROR_CUDA, "compact rows: %s", cudaGetErrorString(cudaGetLastError()));
+  if (st || (scoo && (hflag[0] & 1u))) {  // an offset does not fit: 32-bit rows
     cudaFree(blk);
     return st;
   }
-  m->rel = rel;
+  if (w == 1) m->rel8 = blk, m->wide_tiles = hflag[1];
+  else m->rel = reinterpret_cast<uint16_t *>(blk);
   m->tile_base = base;
   m->allocs.push_back(blk);
   m->device_bytes += rel_bytes + (size_t)tiles * 4;
-  m->format_bytes -= (uint64_t)n * 2;
-  m->format_bytes += (uint64_t)tiles * 4;
+  // bytes a launch reads for the rows: w per element, 4 per tile base, and
+  // 4 - w more per element of a wide tile
+  m->format_bytes -= (uint64_t)n * (4u - w);
+  m->format_bytes += (uint64_t)tiles * 4 + (w == 1 ? (uint64_t)hflag[1] * d::kWarpTile * 3u : 0u);
   return ok();
 }
 
@@ -1841,9 +1871,11 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
                                    (float *)y, stream);
     case MFP_FORMAT_COO:
       return f64 ? coo_spmv<double>(m->rows, (uint32_t)m->nnz, (const double *)m->vals, m->cols_a, m->rows_a,
-                                    (const double *)x, (double *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base)
+                                    (const double *)x, (double *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base,
+                                    m->rel8, m->wide_tiles > 0)
                  : coo_spmv<float>(m->rows, (uint32_t)m->nnz, (const float *)m->vals, m->cols_a, m->rows_a,
-                                   (const float *)x, (float *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base);
+                                   (const float *)x, (float *)y, m->ws, m->ws_bytes, stream, m->rel, m->tile_base,
+                                   m->rel8, m->wide_tiles > 0);
     case MFP_FORMAT_SCOO:
       if (m->rows_unsorted)
         return f64 ? scoo_spmv<double, true>(m->rows, m->slices, m->slice_size, (const double *)m->vals, m->cols_a,
@@ -1861,10 +1893,10 @@ int mfp_matrix_spmv(const mfp_matrix *m, const void *x, void *y, void *stream) {
     case MFP_FORMAT_HYBRID:
       return f64 ? hyb_spmv<double>(m->rows, m->width, (const double *)m->vals, m->cols_a, m->coo_nnz,
                                     (const double *)m->vals2, m->cols2, m->rows2, (const double *)x, (double *)y,
-                                    m->ws, m->ws_bytes, stream, m->rel, m->tile_base)
+                                    m->ws, m->ws_bytes, stream, m->rel, m->tile_base, m->rel8, m->wide_tiles > 0)
                  : hyb_spmv<float>(m->rows, m->width, (const float *)m->vals, m->cols_a, m->coo_nnz,
                                    (const float *)m->vals2, m->cols2, m->rows2, (const float *)x, (float *)y, m->ws,
-                                   m->ws_bytes, stream, m->rel, m->tile_base);
+                                   m->ws_bytes, stream, m->rel, m->tile_base, m->rel8, m->wide_tiles > 0);
     case MFP_FORMAT_ELL_LOWP:
       return lowp_ell_spmv(m->lowp_vt, m->rows, m->cols, m->width, (const uint16_t *)m->vals, m->scale,
                            m->delta ? nullptr : m->cols_a, m->delta, (const float *)x, (float *)y, stream);

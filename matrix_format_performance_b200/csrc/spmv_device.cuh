@@ -87,6 +87,17 @@ __device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t *p, uint64_t po
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
   return v;
 }
+// 8 bytes (p 8-byte aligned) and one byte, streamed like the above.
+__device__ __forceinline__ void ld_stream8_u8(const uint8_t *p, uint32_t (&w)[2], uint64_t pol) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+               : "=r"(w[0]), "=r"(w[1])
+               : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ uint32_t ld_stream_u8(const uint8_t *p, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
 
 // 32-byte store (p 32-byte aligned).
 __device__ __forceinline__ void st_global8(float *p, const float (&v)[8]) {

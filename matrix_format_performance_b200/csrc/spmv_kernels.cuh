@@ -1220,19 +1220,88 @@ __device__ __forceinline__ uint32_t load_run_group16(const T *__restrict__ vals,
   return cnt;
 }
 
-// Compact COO rows: rows[e] - rows[first element of e's 256-element tile],
-// and that first row per tile; *flag |= 1 when a tile spans more than 65,535
-// rows (the layout then keeps 32-bit rows).  rows sorted.
+// A group of 8 elements whose rows are 8-bit offsets rel from a base row
+// (compact COO rows of tiles that span at most 256 rows): as
+// load_run_group16, with one 8-byte load for the offsets.
+template <typename T, int VEC, typename XS>
+__device__ __forceinline__ uint32_t load_run_group8(const T *__restrict__ vals, const uint32_t *__restrict__ cols,
+                                                    const uint8_t *__restrict__ rel, uint32_t base, XS xs,
+                                                    uint32_t g, uint32_t c0, uint32_t c1, T (&p)[kEpt],
+                                                    uint32_t (&r)[kEpt], uint32_t &i0, uint64_t pol) {
+  i0 = max(g, c0);
+  const uint32_t i1 = min(g + kEpt, c1);
+  if (i0 >= i1) return 0u;
+  const uint32_t cnt = i1 - i0;
+  if (VEC == 2 && cnt == kEpt) {
+    T v[8];
+    uint32_t k[8], w[2];
+    ld_stream8(vals + i0, v, pol);
+    ld_stream8(cols + i0, k, pol);
+    ld_stream8_u8(rel + i0, w, pol);
+    T xv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xv[j] = xs(k[j]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      p[j] = mul_rn(v[j], xv[j]);
+      r[j] = base + ((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
+    }
+  } else {
+#pragma unroll
+    for (uint32_t k = 0; k < kEpt; ++k) {
+      if (k < cnt) {
+        const uint32_t e = i0 + k;
+        r[k] = base + ld_stream_u8(rel + e, pol);
+        p[k] = mul_rn(ld_stream1(vals + e, pol), xs(ld_stream1(cols + e, pol)));
+      }
+    }
+  }
+  return cnt;
+}
+
+// Compact COO rows.  Step 1, one warp per 256-element tile: the tile's
+// widest offset rows[e] - rows[tile's first element] (unsigned: an unsorted
+// row counts as wide).  flag[0] |= 1 when some offset exceeds 65,535 (no
+// 16-bit layout); flag[1] counts the tiles with an offset above 255.
+__global__ void coo_rows_span_kernel(uint32_t nnz, const uint32_t *__restrict__ rows, uint32_t *flag) {
+  const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+  if ((uint64_t)t * kWarpTile >= nnz) return;  // whole warps
+  const uint32_t c0 = t * kWarpTile, c1 = min(nnz, c0 + kWarpTile), base = rows[c0];
+  uint32_t dmax = 0;
+  for (uint32_t e = c0 + lane; e < c1; e += 32u) dmax = max(dmax, rows[e] - base);
+  dmax = __reduce_max_sync(0xffffffffu, dmax);
+  if (lane == 0 && dmax > 0xffffu) atomicOr(flag, 1u);
+  if (lane == 0 && dmax > 0xffu) atomicAdd(flag + 1, 1u);
+}
+
+// 8-bit layout, tile_base bit 31: the tile spans more than 256 rows and its
+// rows come from the 32-bit array (rows below 2^31 only).
+constexpr uint32_t kWideTile = 0x80000000u;
+
+// Step 2, 8-bit layout (one warp per tile): each element's offset from its
+// tile's first row, and that row per tile, marked kWideTile (offsets left 0)
+// when an offset does not fit.
+__global__ void coo_rows8_kernel(uint32_t nnz, const uint32_t *__restrict__ rows, uint32_t *__restrict__ tile_base,
+                                 uint8_t *__restrict__ rel) {
+  const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+  if ((uint64_t)t * kWarpTile >= nnz) return;
+  const uint32_t c0 = t * kWarpTile, c1 = min(nnz, c0 + kWarpTile), base = rows[c0];
+  uint32_t dmax = 0;
+  for (uint32_t e = c0 + lane; e < c1; e += 32u) dmax = max(dmax, rows[e] - base);
+  const bool wide = __reduce_max_sync(0xffffffffu, dmax) > 0xffu;
+  for (uint32_t e = c0 + lane; e < c1; e += 32u) rel[e] = wide ? 0u : (uint8_t)(rows[e] - base);
+  if (lane == 0) tile_base[t] = base | (wide ? kWideTile : 0u);
+}
+
+// Step 2, 16-bit layout (every offset fits): offsets and the first row per tile.
 __global__ void coo_rows16_kernel(uint32_t nnz, const uint32_t *__restrict__ rows, uint32_t *__restrict__ tile_base,
-                                  uint16_t *__restrict__ rel, uint32_t *flag) {
+                                  uint16_t *__restrict__ rel) {
   const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nnz) return;
   const uint32_t t = e / kWarpTile;
   const uint32_t base = rows[t * kWarpTile];
-  const uint32_t d = rows[e] - base;
   if (e % kWarpTile == 0) tile_base[t] = base;
-  if (d > 0xffffu) atomicOr(flag, 1u);
-  rel[e] = (uint16_t)d;
+  rel[e] = (uint16_t)(rows[e] - base);
 }
 
 // Compact SCOO rows: r_index[e] - s * slice_size for the elements of slice s
@@ -1248,13 +1317,14 @@ __global__ void scoo_rows16_kernel(uint32_t slice_size, const uint32_t *__restri
   }
 }
 
-// R16: rows as 16-bit offsets rel from tile_base[tile] (compact COO rows).
-template <typename T, int VEC, bool ACCUM, bool R16 = false>
+// R16 / R8: rows as 16-bit offsets rel / 8-bit offsets rel8 from
+// tile_base[tile] (compact COO rows; R8 with WIDE: some tiles read rows).
+template <typename T, int VEC, bool ACCUM, bool R16 = false, bool R8 = false, bool WIDE = false>
 __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : MFP_COO_MINBLOCKS64)
     coo_warp_kernel(uint32_t n_rows, uint32_t nnz, const T *__restrict__ vals, const uint32_t *__restrict__ cols,
                     const uint32_t *__restrict__ rows, const T *__restrict__ x, T *__restrict__ y,
                     coo_carry<T> cw, coo_ws_header *hdr, const uint16_t *__restrict__ rel = nullptr,
-                    const uint32_t *__restrict__ tile_base = nullptr) {
+                    const uint32_t *__restrict__ tile_base = nullptr, const uint8_t *__restrict__ rel8 = nullptr) {
   if (ACCUM) griddep_wait();  // y holds the ELL part written by the preceding launch
   const uint64_t pol = policy_evict_first();
   const uint32_t lane = threadIdx.x & 31u;
@@ -1264,7 +1334,29 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? MFP_COO_MINBLOCKS : M
   T pr[kEpt];
   uint32_t rw[kEpt], i0 = 0;
   uint32_t cnt, prv, nxt;
-  if (R16) {
+  if (R8) {
+    // WIDE: a tile marked kWideTile takes its rows from the 32-bit array; its
+    // loads go out after the gathers, so other tiles wait for nothing extra
+    const uint32_t tb = __ldg(tile_base + wt);
+    cnt = load_run_group8<T, VEC>(vals, cols, rel8, WIDE ? tb & ~kWideTile : tb, x_global<T>{x}, c0 + lane * kEpt,
+                                  c0, c1, pr, rw, i0, pol);
+    if (WIDE && (tb & kWideTile)) {
+#pragma unroll
+      for (uint32_t k = 0; k < kEpt; ++k)
+        if (k < cnt) rw[k] = __ldg(rows + i0 + k);
+    }
+    if (WIDE) {
+      prv = kNoRow;  // row before the tile
+      if (c0 > 0) {
+        const uint32_t pb = __ldg(tile_base + wt - 1u);
+        prv = (pb & kWideTile) ? __ldg(rows + c0 - 1u) : pb + ld_stream_u8(rel8 + c0 - 1u, pol);
+      }
+      nxt = c1 < nnz ? __ldg(tile_base + wt + 1u) & ~kWideTile : kNoRow;  // the next tile's first row
+    } else {
+      prv = c0 > 0 ? __ldg(tile_base + wt - 1u) + ld_stream_u8(rel8 + c0 - 1u, pol) : kNoRow;
+      nxt = c1 < nnz ? __ldg(tile_base + wt + 1u) : kNoRow;
+    }
+  } else if (R16) {
     cnt = load_run_group16<T, VEC>(vals, cols, rel, __ldg(tile_base + wt), x_global<T>{x}, c0 + lane * kEpt, c0, c1,
                                    pr, rw, i0, pol);
     prv = c0 > 0 ? __ldg(tile_base + wt - 1u) + ld_stream_u16(rel + c0 - 1u, pol) : kNoRow;  // row before the tile

@@ -353,14 +353,56 @@ def test_scoo_tiles_and_chunk_fallback(oracle_lib, dtype):
     check_tol(oracle_lib, m, x, a, "scoo tiles / chunks")
 
 
+def compact_row_bytes(rows, dtype):
+    """(bytes per row id, wide tiles) of a COO handle: 1 when at most one
+    256-element tile in 8 spans more than 256 rows (those wide tiles read
+    4-byte rows; float32 only, float64 needs none), else 2 when every tile
+    spans at most 65,536 rows, else 4."""
+    rows = np.asarray(rows, np.int64)
+    if rows.size == 0:
+        return 4, 0
+    span = np.maximum.reduceat(rows - np.repeat(rows[::256], 256)[:rows.size], np.arange(0, rows.size, 256))
+    wide = int((span > 0xFF).sum())
+    if wide <= span.size // 8 and (wide == 0 or np.dtype(dtype) == np.float32):
+        return 1, wide
+    return (2 if span.max() <= 0xFFFF else 4), 0
+
+
+def gapped_rows_matrix(dtype, gap, holes=()):
+    """Rows of 4-8 elements separated by `gap` - 1 empty rows (a 256-element
+    tile spans about 43 * gap rows), and no elements in the row ranges
+    `holes` (start, length)."""
+    rng = np.random.default_rng(11)
+    rows, cols = 200_000, 5000
+    lens = np.zeros(rows, np.int64)
+    lens[::gap] = rng.integers(4, 9, lens[::gap].size)
+    for a, n in holes:
+        lens[a:a + n] = 0
+    rp = np.zeros(rows + 1, np.uint32)
+    rp[1:] = np.cumsum(lens)
+    colv = np.concatenate([np.sort(rng.choice(cols, n, replace=False)) for n in lens if n]).astype(np.uint32)
+    return F.csr_matrix_class.from_arrays(rows, cols, rp, colv, rng.uniform(-1, 1, colv.size), dtype)
+
+
+COMPACT_CASES = {"gap_3": (3, ()), "gap_200": (200, ()),
+                 "holes": (1, ((5_000, 300), (50_000, 1_000), (120_000, 70_000), (199_000, 500)))}
+
+
+@pytest.mark.parametrize("case", ["power_law_300k", "gap_3", "gap_200", "holes"])
 @pytest.mark.parametrize("fmt", [COO, SCOO, HYBRID])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_compact_rows_give_the_bits_of_32_bit_rows(oracle_lib, fmt, dtype):
-    """COO, SCOO and hybrid handles keep their rows as 16-bit offsets (from
-    each 256-element tile's first row, or the slice's first row): the same
-    bits as the raw entry points on the 32-bit row ids, and 2 bytes less
-    per row id in the handle's byte count."""
-    m = syn("power_law_300k").astype(dtype)
+def test_compact_rows_give_the_bits_of_32_bit_rows(oracle_lib, case, fmt, dtype):
+    """COO, SCOO and hybrid handles keep their rows as offsets.  COO and the
+    hybrid's tail: 8-bit offsets from each 256-element tile's first row when
+    at most one tile in 8 spans more than 256 rows, those wide tiles reading
+    the 32-bit rows (the power-law matrix; rows with 2 empty rows between
+    them; in float32, empty row ranges of 300 to 70,000 rows, which also
+    make one tile span more than 65,536 rows: 32-bit rows in float64), else
+    16-bit (199 empty rows between rows).
+    SCOO: 16-bit offsets from the slice's first row.  The same bits as the
+    raw entry points on the 32-bit row ids, and the handle's byte count
+    charges the row bytes read."""
+    m = syn(case).astype(dtype) if case == "power_law_300k" else gapped_rows_matrix(dtype, *COMPACT_CASES[case])
     x = synth.vector(13, m.cols).astype(dtype)
     xt = torch.from_numpy(x).cuda()
     sfx = "f32" if dtype == np.float32 else "f64"
@@ -411,7 +453,12 @@ def test_compact_rows_give_the_bits_of_32_bit_rows(oracle_lib, fmt, dtype):
     assert np.array_equal(yr.cpu().numpy().view(np.uint8), yh.cpu().numpy().view(np.uint8))
     check_tol(oracle_lib, m, x, yh.cpu().numpy(), "compact rows")
     if fmt == COO:
-        assert info.format_bytes == m.nnz * (vs + 6) + 4 * tiles + m.cols * vs + m.rows * vs
+        rb, wide = compact_row_bytes(c.rows_, dtype)
+        holes64 = case == "holes" and dtype == np.float64  # a tile spans 70,043 rows: 32-bit rows
+        assert rb == (2 if case == "gap_200" else 4 if holes64 else 1)
+        assert (wide > 0) == (case == "holes" and dtype == np.float32)
+        assert info.format_bytes == (m.nnz * (vs + 4 + rb) + (4 * tiles if rb < 4 else 0) + wide * 256 * 3
+                                     + m.cols * vs + m.rows * vs)
     elif fmt == SCOO:
         assert info.format_bytes == m.nnz * (vs + 6) + (c.slices_count + 1) * 4 + m.cols * vs + m.rows * vs
 
