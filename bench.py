@@ -276,10 +276,11 @@ def measure_plain(name, m, formats, steps, warmup, flush, stream, peak, hybrid_w
             "formats": out, "fastest": min(out, key=lambda k: out[k]["ms"])}
 
 
-def byte_model_width(m, vs: int, row_bytes: int = 2, cap: int = 64) -> int:
+def byte_model_width(m, vs: int, row_bytes: int = 1, cap: int = 64) -> int:
     """The hybrid ELL width that moves the fewest bytes: w slots of (value,
-    column) for every row against (value, column, row offset) for each tail
-    element past w, plus one 4-byte base per 256-element tile of the tail."""
+    column) for every row against (value, column, row offset: 1 byte in a
+    handle's tail) for each tail element past w, plus one 4-byte base per
+    256-element tile of the tail."""
     lens = np.diff(m.row_ptr.astype(np.int64))
     best, best_b = 0, None
     for w in range(0, min(cap, int(lens.max())) + 1):
@@ -615,7 +616,7 @@ def run_extras(args, power_law, x, per_format, flush, stream, peak, hyb_w):
     t = time.time()
     wb = byte_model_width(power_law, 4)
     hw = {"quantile_width": hyb_w, "byte_model_width": wb,
-          "note": "byte model: w*rows*(4+4) + tail*(4+4+2) + tail tiles*4 bytes, minimised over w"}
+          "note": "byte model: w*rows*(4+4) + tail*(4+4+1) + tail tiles*4 bytes, minimised over w"}
     for label, w in (("quantile", hyb_w), ("byte_model", wb)):
         e = measure_plain("power_law_4M", power_law, [HYBRID], steps, warmup, flush, stream, peak, w)
         hw[label] = e["formats"]["GPU Hybrid (atomic)"]

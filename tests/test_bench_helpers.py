@@ -28,7 +28,7 @@ def test_bench_byte_model_width():
 
         def cost(w):
             tail = int(np.maximum(lens - w, 0).sum())
-            return w * m.rows * (vs + 4) + tail * (vs + 6) + (tail + 255) // 256 * 4
+            return w * m.rows * (vs + 4) + tail * (vs + 5) + (tail + 255) // 256 * 4
         w = bench.byte_model_width(m, vs)
         assert cost(w) == min(cost(k) for k in range(0, min(64, int(lens.max())) + 1))
 
