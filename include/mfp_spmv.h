@@ -535,6 +535,13 @@ int mfp_matrix_create_csr(int format, int value_type, uint32_t rows, uint32_t co
                           const mfp_csr_config *config, mfp_matrix **out);
 int mfp_matrix_create_ell(int value_type, uint32_t rows, uint32_t cols, uint32_t width,
                           const uint32_t *ell_columns, const void *ell_data, mfp_matrix **out);
+/* COO (and the hybrid's tail, below): the handle also keeps each row id as a
+ * 1-byte offset from the first row of its 256-element tile (a tile spanning
+ * more than 256 rows reads the 32-bit ids; allowed for at most one tile in 8,
+ * FP32 only), else as a 2-byte offset when every tile spans at most 65,536
+ * rows, else only the 32-bit ids.  The SpMV reads the offsets; the result
+ * bits do not depend on the choice (mfp_matrix_info.format_bytes counts it).
+ * Row-ordered SCOO keeps 2-byte offsets from each slice's first row. */
 int mfp_matrix_create_coo(int value_type, uint32_t rows, uint32_t cols, uint32_t nnz,
                           const uint32_t *coo_rows, const uint32_t *coo_cols,
                           const void *coo_data, mfp_matrix **out);
